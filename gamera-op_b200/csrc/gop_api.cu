@@ -1,0 +1,719 @@
+// C ABI of the B200 MHD step (include/gamera_op.h): instance lifecycle,
+// geometry / PDM-weight tables, host<->device layout conversion and the
+// step sequence.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "gamera_op.h"
+#include "gop_device.cuh"
+#include "gop_kernels.h"
+
+using namespace gop;
+
+namespace {
+
+thread_local char g_err[512] = "";
+
+int fail(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define CK(call)                                                                  \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess)                                                        \
+      return fail(GOP_ECUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                  __LINE__);                                                      \
+  } while (0)
+
+// reference physics constants (src/config.c:82-90)
+constexpr double kGamma = 5.0 / 3.0, kCfl = 0.3, kCa = 10.0, kPdmb = 1.0;
+constexpr double kRhoFloor = 0.00316227, kPFloor = 0.000316227;
+
+// Dense 5x5 LU with partial pivoting and solve (the scheme of
+// math_lib/lu_solver.c:10-104, used by the spherical weights)
+bool lu_solve5(double a[5][5], const double b[5], double x[5]) {
+  int perm[5] = {0, 1, 2, 3, 4};
+  for (int k = 0; k < 4; k++) {
+    int piv = k;
+    double best = std::fabs(a[k][k]);
+    for (int i = k + 1; i < 5; i++)
+      if (std::fabs(a[i][k]) > best) {
+        best = std::fabs(a[i][k]);
+        piv = i;
+      }
+    if (best < 1e-12) return false;
+    if (piv != k) {
+      for (int j = 0; j < 5; j++) std::swap(a[k][j], a[piv][j]);
+      std::swap(perm[k], perm[piv]);
+    }
+    for (int i = k + 1; i < 5; i++) {
+      double m = a[i][k] / a[k][k];
+      a[i][k] = m;
+      for (int j = k + 1; j < 5; j++) a[i][j] -= m * a[k][j];
+    }
+  }
+  if (std::fabs(a[4][4]) < 1e-12) return false;
+  double y[5];
+  for (int i = 0; i < 5; i++) {
+    y[i] = b[perm[i]];
+    for (int j = 0; j < i; j++) y[i] -= a[i][j] * y[j];
+  }
+  for (int i = 4; i >= 0; i--) {
+    x[i] = y[i];
+    for (int j = i + 1; j < 5; j++) x[i] -= a[i][j] * x[j];
+    x[i] /= a[i][i];
+  }
+  return true;
+}
+
+double factorial(int k) {
+  double r = 1.0;
+  for (int i = 2; i <= k; ++i) r *= i;
+  return r;
+}
+double choose(int j, int k) {
+  if (k < 0 || k > j) return 0.0;
+  if (k == 0 || k == j) return 1.0;
+  k = std::min(k, j - k);
+  double r = 1.0;
+  for (int i = 1; i <= k; ++i) r *= (j - k + i) / (double)i;
+  return r;
+}
+
+struct Tables {
+  int tmax;
+  std::vector<double> v;
+  double& at(int axis, int t, int idx) { return v[((size_t)axis * NTAB + t) * tmax + idx]; }
+};
+
+// Per-axis geometry, mags interpolation weights, PDM weights and PDM limiter
+// coefficients.  Cartesian formulas: src/cartesian/cartesian_general.c:42-358
+// (the weights scale facPDMU7 by vol/vol_face; on the reference's uniform
+// grid they depend on the transverse position only through round-off, so the
+// tables use the first active transverse cell).  Spherical formulas:
+// src/spherical/spherical_general.c:42-594.
+void build_tables(const gop_desc& d, Tables& T) {
+  const int n[3] = {d.ni, d.nj, d.nk};
+  const double* xs[3] = {d.x1, d.x2, d.x3};
+  int N[3];
+  for (int a = 0; a < 3; a++) N[a] = n[a] + 2 * NGH + 1;
+  T.tmax = std::max(N[0], std::max(N[1], N[2])) + 1;
+  T.v.assign((size_t)3 * NTAB * T.tmax, 0.0);
+  const bool sph = d.coord == GOP_COORD_SPHERICAL;
+  std::vector<double> xctr[3], dxv[3], xcv[3];
+  for (int a = 0; a < 3; a++) {
+    const double* x = xs[a];
+    dxv[a].assign(N[a], 0.0);
+    xcv[a].assign(N[a], 0.0);
+    xctr[a].assign(N[a], 0.0);
+    for (int f = 0; f < N[a]; f++) T.at(a, T_X, f) = x[f];
+    for (int c = 0; c + 1 < N[a]; c++) {
+      dxv[a][c] = x[c + 1] - x[c];
+      xcv[a][c] = 0.5 * (x[c] + x[c + 1]);
+      T.at(a, T_DX, c) = dxv[a][c];
+      double xc = xcv[a][c], dx = dxv[a][c];
+      if (sph && a == 0)
+        xctr[a][c] = xc + 2.0 * xc * dx * dx / (12.0 * xc * xc + dx * dx);
+      else if (sph && a == 1)
+        xctr[a][c] = (std::sin(x[c + 1]) - std::sin(x[c]) -
+                      (x[c + 1] * std::cos(x[c + 1]) - x[c] * std::cos(x[c]))) /
+                     (-std::cos(x[c + 1]) + std::cos(x[c]));
+      else
+        xctr[a][c] = xc;
+      T.at(a, T_MA, c) = (x[c + 1] - xctr[a][c]) / dx;
+      T.at(a, T_MB, c) = (xctr[a][c] - x[c]) / dx;
+    }
+  }
+  if (sph) {
+    const double* r = xs[0];
+    const double* t = xs[1];
+    for (int i = 0; i < N[0]; i++) {
+      T.at(0, T_G0, i) = -r[i] * r[i];
+      if (i + 1 < N[0]) {
+        T.at(0, T_G1, i) = 1.0 / 3.0 * (std::pow(r[i + 1], 3) - std::pow(r[i], 3));
+        T.at(0, T_G2, i) = 0.5 * (r[i + 1] * r[i + 1] - r[i] * r[i]);
+        T.at(0, T_G3, i) = xcv[0][i];
+      }
+    }
+    for (int j = 0; j < N[1]; j++) {
+      T.at(1, T_G1, j) = std::sin(t[j]);
+      if (j + 1 < N[1]) {
+        T.at(1, T_G0, j) = std::cos(t[j + 1]) - std::cos(t[j]);
+        T.at(1, T_G2, j) = std::sin(xcv[1][j]);
+        T.at(1, T_G3, j) = std::sin(t[j + 1]) - std::sin(t[j]);
+        T.at(1, T_G4, j) = std::sin(t[j + 1]) + std::sin(t[j]);
+      }
+    }
+  }
+
+  // PDM geometric factors GF_face / GF_vol along each axis
+  auto gff = [&](int a, int f) -> double {
+    if (!sph) {
+      int o1 = (a + 1) % 3, o2 = (a + 2) % 3;
+      int lo = std::min(o1, o2), hi = std::max(o1, o2);
+      return dxv[lo][NGH] * dxv[hi][NGH];
+    }
+    if (a == 0) return xs[0][f] * xs[0][f];
+    if (a == 1) return std::sin(xs[1][f]);
+    return 1.0;
+  };
+  auto gfv = [&](int a, int f) -> double {
+    if (!sph) {
+      double v[3] = {dxv[0][NGH], dxv[1][NGH], dxv[2][NGH]};
+      v[a] = dxv[a][f];
+      return v[0] * v[1] * v[2];
+    }
+    if (a == 0) return 1.0 / 3.0 * (std::pow(xs[0][f + 1], 3) - std::pow(xs[0][f], 3));
+    if (a == 1) return -(std::cos(xs[1][f + 1]) - std::cos(xs[1][f]));
+    return dxv[2][f];
+  };
+  const double e = 1.0 / (2 * kPdmb + 1.0);
+  static const double fac[7] = {-1.0 / 140.0, 5.0 / 84.0, -101.0 / 420.0, 319.0 / 420.0,
+                                107.0 / 210.0, -19.0 / 210.0, 1.0 / 105.0};
+  static const double f8[8] = {-3.0 / 840, 29.0 / 840, -139.0 / 840, 533.0 / 840,
+                               533.0 / 840, -139.0 / 840, 29.0 / 840, -3.0 / 840};
+  for (int a = 0; a < 3; a++) {
+    for (int f = NGH; f <= NGH + n[a]; f++) {
+      // limiter coefficients of the left (cell f-1) and right (cell f) states
+      double q = gfv(a, f - 1) / dxv[a][f - 1], f0 = gff(a, f), fm = gff(a, f - 1);
+      T.at(a, T_CL1, f) = (q - e * f0) / (e * f0);
+      T.at(a, T_CL2, f) = (e * fm - q) / (e * f0);
+      q = gfv(a, f) / dxv[a][f];
+      fm = gff(a, f + 1);
+      T.at(a, T_CR1, f) = (q - e * f0) / (e * f0);
+      T.at(a, T_CR2, f) = (e * fm - q) / (e * f0);
+      double wl[7], wr[7];
+      if (!sph) {
+        double vf = 0.0;
+        for (int o = -4; o <= 3; o++) vf += gfv(a, f + o) * f8[o + 4];
+        for (int t = 0; t < 7; t++) wl[t] = wr[t] = fac[t] * gfv(a, f) / vf;
+      } else if (a == 2) {
+        static const double pl[7] = {0.0, 1.0 / 30.0, -13.0 / 60.0, 47.0 / 60.0,
+                                     9.0 / 20.0, -1.0 / 20.0, 0.0};
+        static const double pr[7] = {0.0, -1.0 / 20.0, 9.0 / 20.0, 47.0 / 60.0,
+                                     -13.0 / 60.0, 1.0 / 30.0, 0.0};
+        for (int t = 0; t < 7; t++) {
+          wl[t] = pl[t];
+          wr[t] = pr[6 - t];  // stored w1r..w7r, applied in reverse
+        }
+      } else {
+        // 5-point non-uniform reconstruction from cell averages: radial
+        // moments of r^2 dr, polar moments of sin(theta) dtheta
+        const double* x = xs[a];
+        auto xs_ext = [&](int s) -> double {  // x_s[s] = x[s-4] with linear extension
+          int idx = s - NGH;
+          if (idx < 0) return x[0] + idx * dxv[a][0];
+          if (idx > N[a] - 1) return x[N[a] - 1] + (idx - (N[a] - 1)) * dxv[a][N[a] - 2];
+          return x[idx];
+        };
+        for (int side = 0; side < 2; side++) {
+          double A[5][5], b[5], sol[5];
+          for (int i = -2; i <= 2; i++) {
+            double xm = side == 0 ? xs_ext(f + NGH + i - 1) : xs_ext(f + NGH + i);
+            double xp = side == 0 ? xs_ext(f + NGH + i) : xs_ext(f + NGH + i + 1);
+            for (int j = 0; j <= 4; j++) {
+              if (a == 0) {
+                const int m = 2;
+                A[j][i + 2] = (double)(m + 1) / (double)(j + m + 1) *
+                              (std::pow(xp, j + m + 1) - std::pow(xm, j + m + 1)) /
+                              (std::pow(xp, m + 1) - std::pow(xm, m + 1));
+              } else {
+                double sum = 0.0;
+                for (int k = 0; k <= j; k++)
+                  sum = sum + factorial(k) * choose(j, k) *
+                                  (std::pow(xm, j - k) * std::cos(xm + k * M_PI / 2.0) -
+                                   std::pow(xp, j - k) * std::cos(xp + k * M_PI / 2.0));
+                A[j][i + 2] = sum / (std::cos(xm) - std::cos(xp));
+              }
+            }
+            b[i + 2] = std::pow(xs_ext(f + NGH), i + 2);
+          }
+          double wv[7] = {0, 0, 0, 0, 0, 0, 0};
+          if (lu_solve5(A, b, sol))
+            for (int t = 0; t < 5; t++) wv[t + 1] = sol[t];
+          for (int t = 0; t < 7; t++) {
+            if (side == 0) wl[t] = wv[t];
+            else wr[t] = wv[6 - t];
+          }
+        }
+      }
+      for (int t = 0; t < 7; t++) {
+        T.at(a, T_WL0 + t, f) = wl[t];
+        T.at(a, T_WR0 + t, f) = wr[t];
+      }
+    }
+  }
+}
+
+int check_desc(const gop_desc* d) {
+  if (!d) return fail(GOP_EINVAL, "desc is NULL");
+  if (d->ni < NGH || d->nj < NGH || d->nk < NGH)
+    return fail(GOP_EINVAL, "each axis needs at least %d active cells", NGH);
+  if ((long long)d->ni * d->nj * d->nk > (1LL << 31))
+    return fail(GOP_EINVAL, "grid too large");
+  if (d->coord != GOP_COORD_CARTESIAN && d->coord != GOP_COORD_SPHERICAL)
+    return fail(GOP_EINVAL, "coord must be GOP_COORD_CARTESIAN or GOP_COORD_SPHERICAL");
+  if (!d->x1 || !d->x2 || !d->x3) return fail(GOP_EINVAL, "coordinate arrays are NULL");
+  for (int a = 0; a < 3; a++) {
+    char lo = d->bc[2 * a], hi = d->bc[2 * a + 1];
+    if (!strchr("psrfen", lo) || !strchr("psrfen", hi) || lo == 0 || hi == 0)
+      return fail(GOP_EINVAL, "bad boundary kind on axis %d", a);
+    if ((lo == 'p') != (hi == 'p'))
+      return fail(GOP_EINVAL, "axis %d: periodic must be set on both faces", a);
+  }
+  if (d->precision != GOP_PREC_FP64 && d->precision != GOP_PREC_MIXED)
+    return fail(GOP_EINVAL, "precision must be GOP_PREC_FP64 or GOP_PREC_MIXED");
+  return GOP_OK;
+}
+
+struct Layout {
+  int N[3];
+  int pitch;
+  long long fs;
+};
+
+Layout layout_of(const gop_desc* d) {
+  Layout L;
+  L.N[0] = d->ni + 2 * NGH + 1;
+  L.N[1] = d->nj + 2 * NGH + 1;
+  L.N[2] = d->nk + 2 * NGH + 1;
+  L.pitch = (L.N[0] + 7) / 8 * 8;
+  L.fs = (long long)L.pitch * L.N[1] * L.N[2];
+  return L;
+}
+
+}  // namespace
+
+struct gop_instance {
+  gop_desc d;
+  Params P;
+  cudaStream_t st = nullptr;
+  double* state = nullptr;   // 2 x (6 + 3) fields
+  void* work = nullptr;      // WORK_FIELDS x R
+  double* tab = nullptr;
+  double* scal = nullptr;
+  double* staging = nullptr; // reference-layout scratch, 6 x NI*NJ*NK
+  double* hscal = nullptr;   // pinned host copy of the scalars
+  Work<double> wd;
+  Work<float> wf;
+  size_t bytes = 0;
+  bool prepared = false;
+};
+
+extern "C" {
+
+const char* gop_last_error(void) { return g_err; }
+
+int64_t gop_kernel_launches(void) { return gop::launches(); }
+
+size_t gop_footprint(const gop_desc* d) {
+  if (check_desc(d) != GOP_OK) return 0;
+  Layout L = layout_of(d);
+  size_t rsize = d->precision == GOP_PREC_MIXED ? sizeof(float) : sizeof(double);
+  size_t ref = (size_t)L.N[0] * L.N[1] * L.N[2];
+  size_t tmax = std::max(L.N[0], std::max(L.N[1], L.N[2])) + 1;
+  return (size_t)L.fs * (18 * sizeof(double) + WORK_FIELDS * rsize) + 6 * ref * sizeof(double) +
+         3 * NTAB * tmax * sizeof(double) + NSCAL * sizeof(double);
+}
+
+int gop_create(const gop_desc* desc, gop_instance** out) {
+  if (!out) return fail(GOP_EINVAL, "out is NULL");
+  *out = nullptr;
+  int rc = check_desc(desc);
+  if (rc) return rc;
+  int dev = 0, count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+    return fail(GOP_ENODEV, "no CUDA device");
+  CK(cudaGetDevice(&dev));
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, dev));
+  if (prop.major < 10) return fail(GOP_ENODEV, "device is sm_%d%d; sm_100 required", prop.major, prop.minor);
+
+  gop_instance* h = new (std::nothrow) gop_instance();
+  if (!h) return fail(GOP_ENOMEM, "host allocation failed");
+  h->d = *desc;
+  gop_desc& d = h->d;
+  if (d.gamma == 0) d.gamma = kGamma;
+  if (d.cfl == 0) d.cfl = kCfl;
+  if (d.ca == 0) d.ca = kCa;
+  if (d.rho_floor == 0) d.rho_floor = kRhoFloor;
+  if (d.p_floor == 0) d.p_floor = kPFloor;
+
+  Tables T;
+  build_tables(d, T);
+  Layout L = layout_of(&d);
+  Params& P = h->P;
+  P.n[0] = d.ni;
+  P.n[1] = d.nj;
+  P.n[2] = d.nk;
+  for (int a = 0; a < 3; a++) P.N[a] = L.N[a];
+  P.pitch = L.pitch;
+  P.sj = L.pitch;
+  P.sk = (long long)L.pitch * L.N[1];
+  P.fs = L.fs;
+  P.tmax = T.tmax;
+  P.gamma = d.gamma;
+  P.gm1 = d.gamma - 1.0;
+  P.cfl = d.cfl;
+  P.ca = d.ca;
+  P.ca2 = d.ca * d.ca;
+  P.rho_floor = d.rho_floor;
+  P.p_floor = d.p_floor;
+  P.pdm_a1 = kPdmb / (kPdmb + 1.0);
+  P.pdm_a2 = 1.0 - P.pdm_a1;
+
+  size_t rsize = d.precision == GOP_PREC_MIXED ? sizeof(float) : sizeof(double);
+  size_t ref = (size_t)L.N[0] * L.N[1] * L.N[2];
+  cudaError_t e = cudaSuccess;
+  auto alloc = [&](void** p, size_t bytes) {
+    if (e == cudaSuccess) {
+      e = cudaMalloc(p, bytes);
+      if (e == cudaSuccess) h->bytes += bytes;
+    }
+  };
+  alloc((void**)&h->state, (size_t)L.fs * 18 * sizeof(double));
+  alloc(&h->work, (size_t)L.fs * WORK_FIELDS * rsize);
+  alloc((void**)&h->tab, T.v.size() * sizeof(double));
+  alloc((void**)&h->scal, NSCAL * sizeof(double));
+  alloc((void**)&h->staging, 6 * ref * sizeof(double));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&h->hscal, NSCAL * sizeof(double));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    gop_destroy(h);
+    return fail(GOP_ENOMEM, "device allocation of %zu bytes failed: %s", gop_footprint(&d),
+                cudaGetErrorString(e));
+  }
+  cudaMemset(h->state, 0, (size_t)L.fs * 18 * sizeof(double));
+  cudaMemset(h->work, 0, (size_t)L.fs * WORK_FIELDS * rsize);
+  cudaMemcpy(h->tab, T.v.data(), T.v.size() * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemset(h->scal, 0, NSCAL * sizeof(double));
+  P.tab = h->tab;
+  P.scal = h->scal;
+  P.Wbuf[0] = h->state;
+  P.Bbuf[0] = h->state + 6 * L.fs;
+  P.Wbuf[1] = h->state + 9 * L.fs;
+  P.Bbuf[1] = h->state + 15 * L.fs;
+  if (d.precision == GOP_PREC_MIXED) {
+    float* w = (float*)h->work;
+    h->wf = Work<float>{w, w + 6 * L.fs, w + 9 * L.fs, w + 12 * L.fs, w + 15 * L.fs,
+                        w + 21 * L.fs, w + 24 * L.fs};
+  } else {
+    double* w = (double*)h->work;
+    h->wd = Work<double>{w, w + 6 * L.fs, w + 9 * L.fs, w + 12 * L.fs, w + 15 * L.fs,
+                         w + 21 * L.fs, w + 24 * L.fs};
+  }
+  cudaError_t le = cudaDeviceSynchronize();
+  if (le != cudaSuccess) {
+    gop_destroy(h);
+    return fail(GOP_ECUDA, "initialisation failed: %s", cudaGetErrorString(le));
+  }
+  *out = h;
+  return GOP_OK;
+}
+
+int gop_destroy(gop_instance* h) {
+  if (!h) return GOP_OK;
+  if (h->st) cudaStreamSynchronize(h->st);
+  cudaFree(h->state);
+  cudaFree(h->work);
+  cudaFree(h->tab);
+  cudaFree(h->scal);
+  cudaFree(h->staging);
+  if (h->hscal) cudaFreeHost(h->hscal);
+  delete h;
+  return GOP_OK;
+}
+
+int gop_set_stream(gop_instance* h, void* stream) {
+  if (!h) return fail(GOP_EINVAL, "instance is NULL");
+  h->st = (cudaStream_t)stream;
+  return GOP_OK;
+}
+
+int gop_upload(gop_instance* h, const double* gas, const double* face_b, const double* gas_p,
+               const double* face_b_p, double time, double dt0) {
+  if (!h || !gas || !face_b) return fail(GOP_EINVAL, "NULL argument");
+  if ((gas_p == nullptr) != (face_b_p == nullptr))
+    return fail(GOP_EINVAL, "gas_p and face_b_p go together");
+  const Params& P = h->P;
+  size_t ref = (size_t)P.N[0] * P.N[1] * P.N[2];
+  // the current state goes to buffer 0, the history to buffer 1
+  CK(cudaMemcpyAsync(h->staging, gas, 6 * ref * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  launch_from_ref(P, 6, h->staging, P.Wbuf[0], h->st);
+  CK(cudaMemcpyAsync(h->staging, face_b, 3 * ref * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  launch_from_ref(P, 3, h->staging, P.Bbuf[0], h->st);
+  if (gas_p) {
+    CK(cudaMemcpyAsync(h->staging, gas_p, 6 * ref * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    launch_from_ref(P, 6, h->staging, P.Wbuf[1], h->st);
+    CK(cudaMemcpyAsync(h->staging, face_b_p, 3 * ref * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    launch_from_ref(P, 3, h->staging, P.Bbuf[1], h->st);
+  }
+  double* s = h->hscal;
+  CK(cudaStreamSynchronize(h->st));
+  for (int t = 0; t < NSCAL; t++) s[t] = 0.0;
+  s[S_TIME] = time;
+  s[S_DT0] = dt0;
+  s[S_PAR] = 0.0;
+  CK(cudaMemcpyAsync(h->scal, s, NSCAL * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  h->prepared = false;
+  return GOP_OK;
+}
+
+int gop_prepare(gop_instance* h, int restart) {
+  if (!h) return fail(GOP_EINVAL, "instance is NULL");
+  const Params& P = h->P;
+  // halo + boundary fill of the current state (src/solver_solve.c:25-40)
+  launch_ghosts(P, h->d.bc, 1, h->st);
+  if (!restart) {
+    // AB2 history <- current state (src/solver_solve.c:55-92)
+    CK(cudaMemcpyAsync(P.Wbuf[1], P.Wbuf[0], (size_t)P.fs * 6 * sizeof(double),
+                       cudaMemcpyDeviceToDevice, h->st));
+    CK(cudaMemcpyAsync(P.Bbuf[1], P.Bbuf[0], (size_t)P.fs * 3 * sizeof(double),
+                       cudaMemcpyDeviceToDevice, h->st));
+  }
+  double* s = h->hscal;
+  CK(cudaMemcpyAsync(s, h->scal, NSCAL * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  s[S_NEXT_DT] = DBL_MAX;
+  s[S_DIVB] = 0.0;
+  s[S_STOP] = 0.0;
+  s[S_STEPS] = 0.0;
+  s[S_FLAGS] = 0.0;
+  s[S_PAR] = 0.0;
+  CK(cudaMemcpyAsync(h->scal, s, NSCAL * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  // CFL dt and div B of the initial state (src/solver_solve.c:94-98)
+  launch_dt(P, h->d.coord, h->st);
+  CK(cudaMemcpyAsync(s, h->scal, NSCAL * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  if (!restart) s[S_DT0] = s[S_NEXT_DT];
+  CK(cudaMemcpyAsync(h->scal, s, NSCAL * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  CK(cudaGetLastError());
+  if (!(s[S_NEXT_DT] > 0.0) || s[S_NEXT_DT] >= DBL_MAX)
+    return fail(GOP_ENUMERIC, "initial CFL dt is not positive (%g)", s[S_NEXT_DT]);
+  h->prepared = true;
+  return GOP_OK;
+}
+
+}  // extern "C"
+
+static int enqueue_steps(gop_instance* h, int nsteps, double time_stop) {
+  const Params& P = h->P;
+  launch_arm(P, time_stop, h->st);
+  for (int n = 0; n < nsteps; n++) {
+    launch_begin(P, h->st);
+    if (h->d.precision == GOP_PREC_MIXED)
+      launch_step_body<float>(P, h->d.coord, h->wf, h->st);
+    else
+      launch_step_body<double>(P, h->d.coord, h->wd, h->st);
+    launch_ghosts(P, h->d.bc, 0, h->st);
+    launch_end(P, h->st);
+  }
+  CK(cudaGetLastError());
+  return GOP_OK;
+}
+
+extern "C" {
+
+int gop_step(gop_instance* h, int nsteps, double time_stop, double* time_out) {
+  if (!h) return fail(GOP_EINVAL, "instance is NULL");
+  if (!h->prepared) return fail(GOP_ESTATE, "gop_prepare must run before gop_step");
+  if (nsteps < 0) return fail(GOP_EINVAL, "nsteps < 0");
+  int rc = enqueue_steps(h, nsteps, time_stop);
+  if (rc) return rc;
+  if (time_out) {
+    CK(cudaMemcpyAsync(h->hscal, h->scal, NSCAL * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    *time_out = h->hscal[S_TIME];
+    if (h->hscal[S_FLAGS] != 0.0) return fail(GOP_ENUMERIC, "non-finite or non-positive state");
+  }
+  return GOP_OK;
+}
+
+}  // extern "C"
+
+static int download_field(gop_instance* h, int nf, const double* dev, double* host) {
+  const Params& P = h->P;
+  size_t ref = (size_t)P.N[0] * P.N[1] * P.N[2];
+  launch_to_ref(P, nf, dev, h->staging, h->st);
+  CK(cudaMemcpyAsync(host, h->staging, nf * ref * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return GOP_OK;
+}
+
+template <typename R>
+static int download_work(gop_instance* h, int nf, const R* dev, double* host) {
+  // widen the FP32 work array into a temporary FP64 array first
+  const Params& P = h->P;
+  double* tmp = nullptr;
+  CK(cudaMallocAsync((void**)&tmp, (size_t)P.fs * nf * sizeof(double), h->st));
+  launch_widen<R>(P, nf, dev, tmp, h->st);
+  int rc = download_field(h, nf, tmp, host);
+  cudaFreeAsync(tmp, h->st);
+  CK(cudaStreamSynchronize(h->st));
+  return rc;
+}
+
+extern "C" {
+
+int gop_download(gop_instance* h, double* gas, double* face_b, double* gas_h, double* gas_p,
+                 double* face_b_h, double* face_b_p, double* mags, double* mags_h,
+                 double* mags_p) {
+  if (!h) return fail(GOP_EINVAL, "instance is NULL");
+  const Params& P = h->P;
+  double* s = h->hscal;
+  CK(cudaMemcpyAsync(s, h->scal, NSCAL * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  int cur = s[S_PAR] != 0.0 ? 1 : 0;
+  int rc = GOP_OK;
+  if (gas && (rc = download_field(h, 6, P.Wbuf[cur], gas))) return rc;
+  if (face_b && (rc = download_field(h, 3, P.Bbuf[cur], face_b))) return rc;
+  if (gas_p && (rc = download_field(h, 6, P.Wbuf[1 - cur], gas_p))) return rc;
+  if (face_b_p && (rc = download_field(h, 3, P.Bbuf[1 - cur], face_b_p))) return rc;
+  if (mags) {
+    double* tmp = nullptr;
+    CK(cudaMallocAsync((void**)&tmp, (size_t)P.fs * 3 * sizeof(double), h->st));
+    CK(cudaMemsetAsync(tmp, 0, (size_t)P.fs * 3 * sizeof(double), h->st));
+    launch_mags(P, P.Bbuf[cur], tmp, h->st);
+    rc = download_field(h, 3, tmp, mags);
+    cudaFreeAsync(tmp, h->st);
+    if (rc) return rc;
+  }
+  bool mixed = h->d.precision == GOP_PREC_MIXED;
+  if (gas_h) rc = mixed ? download_work<float>(h, 6, h->wf.Wh, gas_h) : download_field(h, 6, h->wd.Wh, gas_h);
+  if (rc) return rc;
+  if (face_b_h) rc = mixed ? download_work<float>(h, 3, h->wf.Bh, face_b_h) : download_field(h, 3, h->wd.Bh, face_b_h);
+  if (rc) return rc;
+  if (mags_h) rc = mixed ? download_work<float>(h, 3, h->wf.Msh, mags_h) : download_field(h, 3, h->wd.Msh, mags_h);
+  if (rc) return rc;
+  if (mags_p) rc = mixed ? download_work<float>(h, 3, h->wf.Ms, mags_p) : download_field(h, 3, h->wd.Ms, mags_p);
+  CK(cudaGetLastError());
+  return rc;
+}
+
+int gop_get_stats(gop_instance* h, gop_stats* out) {
+  if (!h || !out) return fail(GOP_EINVAL, "NULL argument");
+  double* s = h->hscal;
+  CK(cudaMemcpyAsync(s, h->scal, NSCAL * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  out->time = s[S_TIME];
+  out->dt = s[S_DT];
+  out->dt0 = s[S_DT0];
+  out->divb_max = s[S_DIVB];
+  out->steps = (int64_t)s[S_STEPS];
+  out->flags = s[S_FLAGS] != 0.0 ? 1 : 0;
+  out->reserved = 0;
+  out->device_bytes = h->bytes;
+  return GOP_OK;
+}
+
+
+// ----------------------------------------------------------------- batch
+
+}  // extern "C"
+
+#include <map>
+
+struct gop_batch {
+  std::vector<gop_instance*> m;
+  cudaStream_t st = nullptr;
+  std::vector<cudaStream_t> lanes;
+  std::vector<cudaEvent_t> ev;
+  cudaEvent_t fork = nullptr;
+  std::map<std::vector<int>, cudaGraphExec_t> graphs;
+};
+
+extern "C" {
+
+int gop_batch_create(gop_instance* const* members, int count, gop_batch** out) {
+  if (!members || count <= 0 || !out) return fail(GOP_EINVAL, "bad batch arguments");
+  *out = nullptr;
+  for (int i = 0; i < count; i++) {
+    if (!members[i]) return fail(GOP_EINVAL, "member %d is NULL", i);
+    if (!members[i]->prepared) return fail(GOP_ESTATE, "member %d is not prepared", i);
+  }
+  gop_batch* b = new (std::nothrow) gop_batch();
+  if (!b) return fail(GOP_ENOMEM, "host allocation failed");
+  b->m.assign(members, members + count);
+  CK(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+  b->lanes.resize(count);
+  b->ev.resize(count);
+  for (int i = 0; i < count; i++) {
+    CK(cudaStreamCreateWithFlags(&b->lanes[i], cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&b->ev[i], cudaEventDisableTiming));
+  }
+  *out = b;
+  return GOP_OK;
+}
+
+int gop_batch_destroy(gop_batch* b) {
+  if (!b) return GOP_OK;
+  if (b->st) cudaStreamSynchronize(b->st);
+  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  for (size_t i = 0; i < b->lanes.size(); i++) {
+    cudaStreamDestroy(b->lanes[i]);
+    cudaEventDestroy(b->ev[i]);
+  }
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->st) cudaStreamDestroy(b->st);
+  delete b;
+  return GOP_OK;
+}
+
+// One graph per distinct step vector: each member's steps form an
+// independent branch (fork / join through events), so the small grids of a
+// batch run concurrently from a single graph launch.
+int gop_batch_step(gop_batch* b, const int* steps) {
+  if (!b || !steps) return fail(GOP_EINVAL, "NULL argument");
+  std::vector<int> key(steps, steps + b->m.size());
+  for (int v : key)
+    if (v < 0) return fail(GOP_EINVAL, "negative step count");
+  auto it = b->graphs.find(key);
+  if (it == b->graphs.end()) {
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+    cudaEventRecord(b->fork, b->st);
+    std::vector<cudaStream_t> saved(b->m.size());
+    int rc = GOP_OK;
+    for (size_t i = 0; i < b->m.size() && rc == GOP_OK; i++) {
+      cudaStreamWaitEvent(b->lanes[i], b->fork, 0);
+      saved[i] = b->m[i]->st;
+      b->m[i]->st = b->lanes[i];
+      rc = enqueue_steps(b->m[i], key[i], 1e300);
+      b->m[i]->st = saved[i];
+      cudaEventRecord(b->ev[i], b->lanes[i]);
+      cudaStreamWaitEvent(b->st, b->ev[i], 0);
+    }
+    cudaError_t e = cudaStreamEndCapture(b->st, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return fail(GOP_ECUDA, "graph capture failed: %s", cudaGetErrorString(e));
+    cudaGraphExec_t x = nullptr;
+    e = cudaGraphInstantiate(&x, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(GOP_ECUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
+    it = b->graphs.emplace(key, x).first;
+  }
+  CK(cudaGraphLaunch(it->second, b->st));
+  CK(cudaStreamSynchronize(b->st));
+  return GOP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,186 @@
+// Device-side data layout, geometry and per-face numerics of the GAMERA-OP
+// MHD step on B200 (sm_100a).
+//
+// Layout in HBM: structure of arrays, one 3-D array per field, i fastest,
+// each axis ghost-extended exactly like the reference (n + 2*4 + 1 points,
+// active cells at 4..n+3, the extra point holds the upper boundary face).
+// Rows are padded to a multiple of 8 doubles so every row starts on a
+// 64-byte boundary and warps along i issue coalesced loads.
+//
+// Geometry is separable in both supported coordinate systems, so the device
+// never stores 3-D geometry: face areas, volumes and edge lengths are
+// products of per-axis 1-D tables evaluated in the reference's
+// multiplication order (src/cartesian/cartesian_general.c:42-283,
+// src/spherical/spherical_general.c:42-316).  PDM weights and the PDM
+// limiter's geometric coefficients are per-face 1-D tables.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gop {
+
+constexpr int NGH = 4;
+
+// per-axis 1-D tables (index = position along the axis)
+enum Tab : int {
+  T_X = 0,     // face coordinate x[f]
+  T_DX,        // x[f+1] - x[f]
+  T_MA,        // (x[c+1] - xctr[c]) / dx[c]: weight of the lower face in mags
+  T_MB,        // (xctr[c] - x[c]) / dx[c]: weight of the upper face
+  T_WL0,       // 7 left PDM weights at face f (applied to cells f-4..f+2)
+  T_WR0 = T_WL0 + 7,  // 7 right weights (applied to cells f+3..f-3)
+  T_CL1 = T_WR0 + 7,  // PDM limiter coefficients of the left state
+  T_CL2,
+  T_CR1,       // ... of the right state
+  T_CR2,
+  T_G0,        // coordinate-specific factors (see Geo below)
+  T_G1,
+  T_G2,
+  T_G3,
+  T_G4,
+  NTAB
+};
+
+// device scalars (one double slot each)
+enum Scal : int {
+  S_DT = 0,      // dt of the current step
+  S_DT0,         // dt of the previous step (AB2)
+  S_TIME,        // time_sim
+  S_CAB2,        // 0.5*dt/dt0 of the current step
+  S_NEXT_DT,     // bit pattern of the running CFL minimum (uint64 atomicMin)
+  S_DIVB,        // bit pattern of max|div B| (uint64 atomicMax)
+  S_STEPS,       // steps taken (as double)
+  S_STOP,        // nonzero: time_stop reached, kernels return at once
+  S_TSTOP,       // time_stop of the current gop_step call
+  S_FLAGS,       // bit 0: non-finite / non-positive state seen
+  S_PAR,         // which of the two state buffers holds the current state
+  NSCAL
+};
+
+struct Params {
+  int n[3];           // active cells
+  int N[3];           // ghost-extended points
+  int pitch;          // row pitch (elements)
+  long long sj, sk;   // strides of j and k (stride of i is 1)
+  long long fs;       // stride between fields
+  const double* tab;  // [3][NTAB][tmax]
+  int tmax;
+  double gamma, gm1, cfl, ca, ca2, rho_floor, p_floor;
+  double pdm_a1, pdm_a2;  // PDMB/(PDMB+1), 1-a1
+  double* scal;           // device scalars
+  double* Wbuf[2];        // two 6-field primitive buffers (current / next)
+  double* Bbuf[2];        // two 3-field face-B buffers
+};
+
+__device__ __forceinline__ int cur_buf(const Params& P) { return P.scal[S_PAR] != 0.0 ? 1 : 0; }
+
+__device__ __forceinline__ double tb(const Params& P, int axis, int t, int idx) {
+  return __ldg(P.tab + ((size_t)axis * NTAB + t) * P.tmax + idx);
+}
+
+__device__ __forceinline__ long long lin(const Params& P, int i, int j, int k) {
+  return (long long)k * P.sk + (long long)j * P.sj + i;
+}
+
+__device__ __forceinline__ long long stride(const Params& P, int axis) {
+  return axis == 0 ? 1LL : (axis == 1 ? P.sj : P.sk);
+}
+
+// Geometry policy.  Cartesian: the reference's uniform-grid arrays
+// (dx_a, face_i = dx2*dx3, vol = dx1*dx2*dx3).  Spherical (r, theta, phi):
+// G0..G4 of axis 0 = -r^2, (r1^3-r0^3)/3, (r1^2-r0^2)/2, r_c;
+// of axis 1 = cos(t1)-cos(t0), sin(t), sin(t_c), sin(t1)-sin(t0),
+// sin(t1)+sin(t0).
+template <int COORD>
+struct Geo {
+  __device__ static __forceinline__ double face(const Params& P, int a, int i, int j, int k) {
+    if (COORD == 0) {
+      if (a == 0) return tb(P, 1, T_DX, j) * tb(P, 2, T_DX, k);
+      if (a == 1) return tb(P, 0, T_DX, i) * tb(P, 2, T_DX, k);
+      return tb(P, 0, T_DX, i) * tb(P, 1, T_DX, j);
+    } else {
+      if (a == 0) return tb(P, 0, T_G0, i) * tb(P, 1, T_G0, j) * tb(P, 2, T_DX, k);
+      if (a == 1) return tb(P, 0, T_G2, i) * tb(P, 1, T_G1, j) * tb(P, 2, T_DX, k);
+      return tb(P, 0, T_G2, i) * tb(P, 1, T_DX, j);
+    }
+  }
+  __device__ static __forceinline__ double vol(const Params& P, int i, int j, int k) {
+    if (COORD == 0) return tb(P, 0, T_DX, i) * tb(P, 1, T_DX, j) * tb(P, 2, T_DX, k);
+    return fabs(tb(P, 0, T_G1, i) * tb(P, 1, T_G0, j) * tb(P, 2, T_DX, k));
+  }
+  // edge length of the edge along axis a at (i,j,k)
+  __device__ static __forceinline__ double edge(const Params& P, int a, int i, int j, int k) {
+    if (COORD == 0 || a == 0) return tb(P, a, T_DX, a == 0 ? i : (a == 1 ? j : k));
+    if (a == 1) return tb(P, 0, T_X, i) * tb(P, 1, T_DX, j);
+    return tb(P, 0, T_X, i) * tb(P, 1, T_G1, j) * tb(P, 2, T_DX, k);
+  }
+  // CFL length of cell (i,j,k) along axis a (geo[dxi..dxk])
+  __device__ static __forceinline__ double dl(const Params& P, int a, int i, int j, int k) {
+    if (COORD == 0 || a == 0) return tb(P, a, T_DX, a == 0 ? i : (a == 1 ? j : k));
+    if (a == 1) return tb(P, 0, T_G3, i) * tb(P, 1, T_DX, j);
+    return tb(P, 0, T_G3, i) * tb(P, 1, T_G2, j) * tb(P, 2, T_DX, k);
+  }
+};
+
+template <typename R>
+__device__ __forceinline__ R sgn(R x) {
+  return x > R(0) ? R(1) : (x < R(0) ? R(-1) : R(0));
+}
+
+// PDMU7 (src/solver_func.c:215-253): 7-tap interpolation of the half-step
+// values h[0..6], clamped to the two step-start values adjacent to the face,
+// then the PDM limiter with the geometric reference slope
+// |c1*p0 + c2*pm1|/2 blended with |p0 - pm1|.
+template <typename R>
+__device__ __forceinline__ R pdm7(const R h[7], const R w[7], R pm1, R p0, R pp1, R c1, R c2,
+                                  R a1, R a2) {
+  R fi = h[0] * w[0];
+#pragma unroll
+  for (int t = 1; t < 7; t++) fi = fma(h[t], w[t], fi);
+  R hi = fmax(p0, pp1);
+  R lo = fmin(p0, pp1);
+  R f = fmax(lo, fmin(fi, hi));
+  R d0 = p0 - pm1;
+  R d1 = pp1 - p0;
+  R s1 = sgn(d1);
+  R q0 = fabs(sgn(d0) + s1);
+  R dl = f - p0;
+  R dc = fabs(c1 * p0 + c2 * pm1) * R(0.5);
+  dc = a1 * dc + a2 * fabs(d0);
+  return f - s1 * fmax(R(0), fabs(dl) - q0 * dc);
+}
+
+// Left and right states at face f of a line v[0..7] = cells f-4..f+3, with
+// the limiter on lim[0..3] = cells f-2..f+1.
+template <typename R>
+struct FaceWeights {
+  R wl[7], wr[7], cl1, cl2, cr1, cr2;
+};
+
+template <typename R>
+__device__ __forceinline__ void load_weights(const Params& P, int axis, int f, FaceWeights<R>& W) {
+#pragma unroll
+  for (int t = 0; t < 7; t++) {
+    W.wl[t] = (R)tb(P, axis, T_WL0 + t, f);
+    W.wr[t] = (R)tb(P, axis, T_WR0 + t, f);
+  }
+  W.cl1 = (R)tb(P, axis, T_CL1, f);
+  W.cl2 = (R)tb(P, axis, T_CL2, f);
+  W.cr1 = (R)tb(P, axis, T_CR1, f);
+  W.cr2 = (R)tb(P, axis, T_CR2, f);
+}
+
+template <typename R>
+__device__ __forceinline__ void recon_lr(const R v[8], const R lim[4], const FaceWeights<R>& W,
+                                         R a1, R a2, R& L, R& Rr) {
+  // left: cells f-4..f+2, limiter cells f-2 (im1), f-1 (i0), f (ip1)
+  L = pdm7<R>(v, W.wl, lim[0], lim[1], lim[2], W.cl1, W.cl2, a1, a2);
+  // right: cells f+3..f-3, limiter f+1 (im1), f (i0), f-1 (ip1)
+  R h[7];
+#pragma unroll
+  for (int t = 0; t < 7; t++) h[t] = v[7 - t];
+  Rr = pdm7<R>(h, W.wr, lim[3], lim[2], lim[1], W.cr1, W.cr2, a1, a2);
+}
+
+}  // namespace gop

@@ -1,0 +1,39 @@
+// Host-side launchers of the step kernels (implemented in gop_kernels.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "gop_device.cuh"
+
+namespace gop {
+
+// per-step work arrays, each field fs elements, element type R
+template <typename R>
+struct Work {
+  R* Wh;   // 6 half-step primitives
+  R* Ms;   // 3 cell-centred B at step start (PDM limiter reference)
+  R* Msh;  // 3 half-step cell-centred B
+  R* Bh;   // 3 half-step face fields
+  R* V;    // 6 centre-to-edge first-sweep velocities (2 per edge direction)
+  R* E;    // 3 edge EMFs
+  R* F;    // 27 face fluxes (9 per direction)
+};
+constexpr int WORK_FIELDS = 6 + 3 + 3 + 3 + 6 + 3 + 27;
+
+int64_t launches();
+void launch_begin(const Params& P, cudaStream_t st);
+void launch_end(const Params& P, cudaStream_t st);
+void launch_arm(const Params& P, double tstop, cudaStream_t st);
+void launch_dt(const Params& P, int coord, cudaStream_t st);
+template <typename R>
+void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t st);
+// which = 0: the buffer being written this step; 1: the current state
+void launch_ghosts(const Params& P, const char bc[6], int which, cudaStream_t st);
+void launch_from_ref(const Params& P, int nf, const double* src, double* dst, cudaStream_t st);
+void launch_to_ref(const Params& P, int nf, const double* src, double* dst, cudaStream_t st);
+template <typename R>
+void launch_widen(const Params& P, int nf, const R* src, double* dst, cudaStream_t st);
+void launch_mags(const Params& P, const double* B, double* out, cudaStream_t st);
+
+}  // namespace gop

@@ -1,0 +1,180 @@
+/*
+ * gamera_op.h -- C ABI of the B200 implementation of GAMERA-OP's
+ * single-domain MHD time step.
+ *
+ * The reference exposes its step as C globals plus `int solve(int nt)`
+ * (src/solver.h:65, src/solver_solve.c:23-536) driven by `main`
+ * (src/main.c:75).  These entry points are what a replacement `solve()`
+ * binds to: the host keeps its config.yaml, problem hooks
+ * (src/problem.h:5-12), boundary library (src/boundary_conditions.c) and
+ * HDF5 output (src/hdf5_io.c:353-523); the state lives on the GPU between
+ * output times.  Plain pointers and sizes only; every call returns 0 on
+ * success or a negative GOP_E* code, and never aborts.
+ *
+ * Array layout at this boundary is the reference's own: field-major, then
+ * i, j, k with k fastest, every axis ghost-extended to n + 2*4 + 1 points
+ * (src/config.h:10, src/config.c:184-186, src/array.c:87-114).
+ */
+#ifndef GAMERA_OP_H
+#define GAMERA_OP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GOP_ABI_VERSION 1
+
+/* error codes */
+#define GOP_OK 0
+#define GOP_EINVAL (-22)   /* bad argument */
+#define GOP_ENOMEM (-12)   /* device allocation failed */
+#define GOP_ECUDA (-5)     /* CUDA runtime error (see gop_last_error) */
+#define GOP_ENODEV (-19)   /* no usable sm_100 device */
+#define GOP_ESTATE (-71)   /* call out of order (e.g. step before prepare) */
+#define GOP_ENUMERIC (-34) /* non-finite or non-positive state detected */
+#define GOP_EBUSY (-16)    /* admission refused: memory budget exceeded */
+
+/* coordinate systems: COORD_TYPE of CMakeLists.txt:77-95 */
+#define GOP_COORD_CARTESIAN 0
+#define GOP_COORD_SPHERICAL 2
+
+/* ghost-fill kinds per face, the library of src/boundary_conditions.c plus
+ * the periodic halo of src/boundary_exchange.c */
+#define GOP_BC_PERIODIC 'p'
+#define GOP_BC_SYMMETRIC 's'
+#define GOP_BC_REFLECTIVE 'r'
+#define GOP_BC_FIXED 'f'
+#define GOP_BC_EXTRAPOLATED 'e'
+#define GOP_BC_NONE 'n'
+
+/* arithmetic of the reconstruction / Riemann flux / edge-EMF stages */
+#define GOP_PREC_FP64 0  /* plain: everything in FP64 (reference parity) */
+#define GOP_PREC_MIXED 1 /* FP32 stages, FP64 state, AB2 and p recovery */
+
+typedef struct {
+  int ni, nj, nk;     /* active cells (config.ni/nj/nk), each >= 4 */
+  int coord;          /* GOP_COORD_* */
+  const double *x1;   /* face coordinates incl. ghosts: ni+9 values, x1[i][0][0] */
+  const double *x2;   /* nj+9 values, x2[0][j][0] */
+  const double *x3;   /* nk+9 values, x3[0][0][k] */
+  char bc[6];         /* faces i-lo,i-hi,j-lo,j-hi,k-lo,k-hi (GOP_BC_*) */
+  int precision;      /* GOP_PREC_* */
+  /* physics constants of src/config.c:82-97 (0 selects the default) */
+  double gamma;       /* 5/3 */
+  double cfl;         /* 0.3 */
+  double ca;          /* Boris speed of light CA, 10 */
+  double rho_floor;   /* 0.00316227 */
+  double p_floor;     /* 0.000316227 */
+} gop_desc;
+
+typedef struct {
+  double time;       /* time_sim */
+  double dt;         /* dt of the last step */
+  double dt0;        /* dt0 (previous dt, AB2 history) */
+  double divb_max;   /* divB_max of the current state (src/solver_func.c:324-343) */
+  int64_t steps;     /* steps taken since prepare */
+  int32_t flags;     /* nonzero: non-finite or non-positive state was seen */
+  int32_t reserved;
+  size_t device_bytes; /* device memory held by this instance */
+} gop_stats;
+
+typedef struct gop_instance gop_instance;
+
+/* Replaces allocate_solver + set_geometry_arrays + getweights
+ * (src/solver_init.c:378-392,471-476; src/main.c:56): allocates device
+ * state and builds geometry and PDM weight tables from the coordinates. */
+int gop_create(const gop_desc *desc, gop_instance **out);
+int gop_destroy(gop_instance *h);
+
+/* Device bytes gop_create would allocate for desc (admission control). */
+size_t gop_footprint(const gop_desc *desc);
+
+/* Runs the instance's work on this CUDA stream (cudaStream_t as void*;
+ * NULL = default stream). */
+int gop_set_stream(gop_instance *h, void *stream);
+
+/* Copies the primitive state into the instance.  gas: 6 fields
+ * rho,v1,v2,v3,p,p_S ([6][NI][NJ][NK], the store slots gas[0][0..5]);
+ * face_b: 3 fields mag_bi,mag_bj,mag_bk ([3][NI][NJ][NK], gem[0..2]).
+ * For a restart also pass the AB2 history gas_p (gas[0][12..17]) and
+ * face_b_p (gem[9..11]) with dt0 and time; otherwise NULL. */
+int gop_upload(gop_instance *h, const double *gas, const double *face_b,
+               const double *gas_p, const double *face_b_p, double time,
+               double dt0);
+
+/* The start of solve() before its loop (src/solver_solve.c:25-99): ghost
+ * fill, derived variables, and for a fresh start (restart == 0) the AB2
+ * history copy and the initial CFL dt0. */
+int gop_prepare(gop_instance *h, int restart);
+
+/* nsteps passes of the time loop (src/solver_solve.c:102-529).  Stops early
+ * once time > time_stop (pass a huge value to disable).  Asynchronous with
+ * respect to the host unless time_out is non-NULL. */
+int gop_step(gop_instance *h, int nsteps, double time_stop, double *time_out);
+
+/* Copies the state back in the reference layout: any pointer may be NULL.
+ * gas/face_b as in gop_upload; gas_h, gas_p (6 fields each) and
+ * face_b_h, face_b_p, mags, mags_h, mags_p (3 fields each) complete the
+ * 18-slot store arrays the per-step HDF5 dump writes
+ * (src/hdf5_io.c:479-508). */
+int gop_download(gop_instance *h, double *gas, double *face_b, double *gas_h,
+                 double *gas_p, double *face_b_h, double *face_b_p,
+                 double *mags, double *mags_h, double *mags_p);
+
+int gop_get_stats(gop_instance *h, gop_stats *out);
+
+/* Last error message of the calling thread ("" if none). */
+const char *gop_last_error(void);
+
+/* Kernels launched by this library since load (for launch accounting). */
+int64_t gop_kernel_launches(void);
+
+/* ---- host-only problem setup (no device work) ------------------------ */
+
+/* Face coordinates of the reference's default uniform grid
+ * (src/solver_init.c:297-321 with one process): n+9 values into x. */
+int gop_grid_uniform(int n, double xmin, double xmax, double *x);
+
+#define GOP_PROBLEM_OT 1        /* src/problem_test_OT_cartesion.c */
+#define GOP_PROBLEM_BLAST 2     /* src/problem_test_Blast_cartesion.c, any centre / field */
+#define GOP_PROBLEM_LOOP_CART 3 /* src/problem_FieldLoop_cartesian.c */
+#define GOP_PROBLEM_LOOP_SPH 4  /* field loop advected through a pole-free spherical shell */
+
+typedef struct {
+  int kind;          /* GOP_PROBLEM_* */
+  double rho;        /* background density */
+  double p_in;       /* blast: pressure inside radius */
+  double p_out;      /* blast: ambient pressure; loops: pressure */
+  double radius;     /* blast radius */
+  double center[3];  /* blast centre */
+  double b[3];       /* blast: uniform face field */
+  double v[3];       /* loops: uniform Cartesian velocity */
+  double loop[4];    /* loop_sph: axis x, axis y, radius R, amplitude A0 */
+} gop_problem;
+
+/* Fills p with the reference problem's values for kind. */
+void gop_problem_defaults(int kind, gop_problem *p);
+
+/* Writes the initial primitive state (6 fields) and face field (3 fields)
+ * of problem p on desc's grid, in the layout of gop_upload.  Ghost cells are
+ * left for gop_prepare to fill, exactly as problem_init leaves them
+ * (src/main.c:57-61). */
+int gop_problem_init(const gop_desc *desc, const gop_problem *p, double *gas, double *face_b);
+
+/* ---- batched stepping of many independent instances ---------------- */
+typedef struct gop_batch gop_batch;
+
+/* Groups instances (all already prepared) so one call advances each by
+ * its own number of steps; launches are captured in a CUDA graph. */
+int gop_batch_create(gop_instance *const *members, int count, gop_batch **out);
+int gop_batch_destroy(gop_batch *b);
+/* steps[m] >= 0 per member; returns when all are done. */
+int gop_batch_step(gop_batch *b, const int *steps);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
