@@ -311,7 +311,54 @@ struct gop_instance {
   Work<float> wf;
   size_t bytes = 0;
   bool prepared = false;
+  // per-kernel-group event timing (gop_set_profiling)
+  bool prof = false;
+  std::vector<cudaEvent_t> pool;
+  struct Rec {
+    int group;
+    cudaEvent_t a, b;
+  };
+  std::vector<Rec> recs;
+  cudaEvent_t open_ev[NGROUP] = {};
+  double prof_ms[NGROUP] = {};
+  int64_t prof_n[NGROUP] = {};
 };
+
+static cudaEvent_t take_event(gop_instance* h) {
+  cudaEvent_t e = nullptr;
+  if (!h->pool.empty()) {
+    e = h->pool.back();
+    h->pool.pop_back();
+  } else {
+    cudaEventCreate(&e);
+  }
+  return e;
+}
+
+static void prof_mark(void* ctx, int group, int start) {
+  gop_instance* h = (gop_instance*)ctx;
+  cudaEvent_t e = take_event(h);
+  cudaEventRecord(e, h->st);
+  if (start) {
+    h->open_ev[group] = e;
+  } else {
+    h->recs.push_back({group, h->open_ev[group], e});
+    h->open_ev[group] = nullptr;
+  }
+}
+
+static void prof_collect(gop_instance* h) {
+  for (auto& r : h->recs) {
+    float ms = 0.f;
+    if (cudaEventSynchronize(r.b) == cudaSuccess && cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+      h->prof_ms[r.group] += ms;
+      h->prof_n[r.group] += 1;
+    }
+    h->pool.push_back(r.a);
+    h->pool.push_back(r.b);
+  }
+  h->recs.clear();
+}
 
 extern "C" {
 
@@ -433,6 +480,8 @@ int gop_destroy(gop_instance* h) {
   cudaFree(h->scal);
   cudaFree(h->staging);
   if (h->hscal) cudaFreeHost(h->hscal);
+  prof_collect(h);
+  for (cudaEvent_t e : h->pool) cudaEventDestroy(e);
   delete h;
   return GOP_OK;
 }
@@ -513,15 +562,26 @@ int gop_prepare(gop_instance* h, int restart) {
 
 static int enqueue_steps(gop_instance* h, int nsteps, double time_stop) {
   const Params& P = h->P;
+  Hook hook;
+  if (h->prof) {
+    hook.mark = prof_mark;
+    hook.ctx = h;
+  }
   launch_arm(P, time_stop, h->st);
   for (int n = 0; n < nsteps; n++) {
+    hook(G_BEGIN, 1);
     launch_begin(P, h->st);
+    hook(G_BEGIN, 0);
     if (h->d.precision == GOP_PREC_MIXED)
-      launch_step_body<float>(P, h->d.coord, h->wf, h->st);
+      launch_step_body<float>(P, h->d.coord, h->wf, h->st, hook);
     else
-      launch_step_body<double>(P, h->d.coord, h->wd, h->st);
+      launch_step_body<double>(P, h->d.coord, h->wd, h->st, hook);
+    hook(G_GHOST, 1);
     launch_ghosts(P, h->d.bc, 0, h->st);
+    hook(G_GHOST, 0);
+    hook(G_END, 1);
     launch_end(P, h->st);
+    hook(G_END, 0);
   }
   CK(cudaGetLastError());
   return GOP_OK;
@@ -603,6 +663,29 @@ int gop_download(gop_instance* h, double* gas, double* face_b, double* gas_h, do
   if (mags_p) rc = mixed ? download_work<float>(h, 3, h->wf.Ms, mags_p) : download_field(h, 3, h->wd.Ms, mags_p);
   CK(cudaGetLastError());
   return rc;
+}
+
+int gop_set_profiling(gop_instance* h, int on) {
+  if (!h) return fail(GOP_EINVAL, "instance is NULL");
+  CK(cudaStreamSynchronize(h->st));
+  prof_collect(h);
+  for (int g = 0; g < NGROUP; g++) {
+    h->prof_ms[g] = 0.0;
+    h->prof_n[g] = 0;
+  }
+  h->prof = on != 0;
+  return GOP_OK;
+}
+
+int gop_get_profile(gop_instance* h, double* ms, int64_t* count) {
+  if (!h || !ms || !count) return fail(GOP_EINVAL, "NULL argument");
+  CK(cudaStreamSynchronize(h->st));
+  prof_collect(h);
+  for (int g = 0; g < NGROUP; g++) {
+    ms[g] = h->prof_ms[g];
+    count[g] = h->prof_n[g];
+  }
+  return GOP_OK;
 }
 
 int gop_get_stats(gop_instance* h, gop_stats* out) {

@@ -743,9 +743,13 @@ void launch_dt(const Params& P, int coord, cudaStream_t st) {
 }
 
 template <typename R>
-void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t st) {
+void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t st,
+                      const Hook& hook) {
   dim3 blk(32, 4, 2);
+  hook(G_AB2, 1);
   LAUNCH(k_ab2<R>, grid3(P.N[0], P.N[1], P.N[2], blk), blk, st, P, w);
+  hook(G_AB2, 0);
+  hook(G_C2C, 1);
   for (int d = 0; d < 3; d++) {
     int p = (d + 1) % 3, q = (d + 2) % 3;
     int cnt[3];
@@ -754,6 +758,8 @@ void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t
     cnt[q] = P.n[q] + 2 * NGH;
     LAUNCH(k_c2c<R>, grid3(cnt[0], cnt[1], cnt[2], blk), blk, st, P, d, w);
   }
+  hook(G_C2C, 0);
+  hook(G_EMF, 1);
   for (int d = 0; d < 3; d++) {
     int p = (d + 1) % 3, q = (d + 2) % 3;
     int cnt[3];
@@ -762,20 +768,27 @@ void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t
     cnt[q] = P.n[q] + 1;
     LAUNCH(k_emf<R>, grid3(cnt[0], cnt[1], cnt[2], blk), blk, st, P, d, w);
   }
+  hook(G_EMF, 0);
+  hook(G_FLUX, 1);
   for (int d = 0; d < 3; d++) {
     int cnt[3] = {P.n[0], P.n[1], P.n[2]};
     cnt[d] += 1;
     LAUNCH(k_flux<R>, grid3(cnt[0], cnt[1], cnt[2], blk), blk, st, P, d, w);
   }
+  hook(G_FLUX, 0);
+  hook(G_UPDATE, 1);
   dim3 ub(32, 4, 2);
   if (coord == 0)
     LAUNCH((k_update<0, R>), grid3(P.n[0], P.n[1], P.n[2], ub), ub, st, P, w);
   else
     LAUNCH((k_update<2, R>), grid3(P.n[0], P.n[1], P.n[2], ub), ub, st, P, w);
+  hook(G_UPDATE, 0);
 }
 
-template void launch_step_body<double>(const Params&, int, const Work<double>&, cudaStream_t);
-template void launch_step_body<float>(const Params&, int, const Work<float>&, cudaStream_t);
+template void launch_step_body<double>(const Params&, int, const Work<double>&, cudaStream_t,
+                                       const Hook&);
+template void launch_step_body<float>(const Params&, int, const Work<float>&, cudaStream_t,
+                                      const Hook&);
 
 void launch_ghosts(const Params& P, const char bc[6], int which, cudaStream_t st) {
   dim3 blk(32, 8, 1);

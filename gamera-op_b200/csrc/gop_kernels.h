@@ -22,12 +22,25 @@ struct Work {
 constexpr int WORK_FIELDS = 6 + 3 + 3 + 3 + 6 + 3 + 27;
 
 int64_t launches();
+
+// kernel groups of one step, for event timing
+enum Group : int { G_BEGIN = 0, G_AB2, G_C2C, G_EMF, G_FLUX, G_UPDATE, G_GHOST, G_END, NGROUP };
+
+// optional timing hook: mark(ctx, group, start) records an event on the stream
+struct Hook {
+  void (*mark)(void* ctx, int group, int start) = nullptr;
+  void* ctx = nullptr;
+  void operator()(int g, int s) const {
+    if (mark) mark(ctx, g, s);
+  }
+};
 void launch_begin(const Params& P, cudaStream_t st);
 void launch_end(const Params& P, cudaStream_t st);
 void launch_arm(const Params& P, double tstop, cudaStream_t st);
 void launch_dt(const Params& P, int coord, cudaStream_t st);
 template <typename R>
-void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t st);
+void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t st,
+                      const Hook& hook = Hook());
 // which = 0: the buffer being written this step; 1: the current state
 void launch_ghosts(const Params& P, const char bc[6], int which, cudaStream_t st);
 void launch_from_ref(const Params& P, int nf, const double* src, double* dst, cudaStream_t st);

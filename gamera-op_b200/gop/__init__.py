@@ -89,6 +89,8 @@ def lib():
         L.gop_grid_uniform.argtypes = [C.c_int, C.c_double, C.c_double, _dp]
         L.gop_problem_defaults.argtypes = [C.c_int, C.POINTER(Problem)]
         L.gop_problem_init.argtypes = [C.POINTER(Desc), C.POINTER(Problem), _dp, _dp]
+        L.gop_set_profiling.argtypes = [vp, C.c_int]
+        L.gop_get_profile.argtypes = [vp, _dp, C.POINTER(C.c_int64)]
         L.gop_batch_create.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(vp)]
         L.gop_batch_destroy.argtypes = [vp]
         L.gop_batch_step.argtypes = [vp, C.POINTER(C.c_int)]
@@ -215,6 +217,18 @@ class Instance:
                 args.append(None)
         _check(lib().gop_download(self._h, *args))
         return out
+
+    GROUPS = ("begin", "ab2", "c2c", "emf", "flux", "update", "ghost", "end")
+
+    def set_profiling(self, on: bool):
+        _check(lib().gop_set_profiling(self._h, int(bool(on))))
+
+    def profile(self) -> dict:
+        """Summed event-timed milliseconds and occurrence count per kernel group."""
+        ms = np.zeros(len(self.GROUPS))
+        cnt = (C.c_int64 * len(self.GROUPS))()
+        _check(lib().gop_get_profile(self._h, _ptr(ms), cnt))
+        return {g: (float(ms[i]), int(cnt[i])) for i, g in enumerate(self.GROUPS)}
 
     def stats(self) -> dict:
         s = Stats()

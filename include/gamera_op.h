@@ -126,6 +126,15 @@ int gop_download(gop_instance *h, double *gas, double *face_b, double *gas_h,
 
 int gop_get_stats(gop_instance *h, gop_stats *out);
 
+/* Diagnostics: time every kernel group of every step with CUDA events on
+ * the instance's stream (off by default; switching resets the totals).
+ * Groups: 0 begin, 1 ab2, 2 centre-to-edge, 3 edge EMF, 4 face flux,
+ * 5 update, 6 ghost fill, 7 end.  ms[g] and count[g] (GOP_NGROUP entries)
+ * are the summed milliseconds and the number of timed occurrences. */
+#define GOP_NGROUP 8
+int gop_set_profiling(gop_instance *h, int on);
+int gop_get_profile(gop_instance *h, double *ms, int64_t *count);
+
 /* Last error message of the calling thread ("" if none). */
 const char *gop_last_error(void);
 
