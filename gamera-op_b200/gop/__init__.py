@@ -203,15 +203,21 @@ class Instance:
         _check(lib().gop_step(self._h, int(nsteps), ts, C.byref(t) if sync else None))
         return t.value if sync else None
 
-    def download(self, which=("gas", "face_b")):
+    def download(self, which=("gas", "face_b"), out=None):
+        """Copies fields back; ``out`` may supply destination arrays (e.g.
+        pinned host buffers) keyed by field name."""
         names = ["gas", "face_b", "gas_h", "gas_p", "face_b_h", "face_b_p", "mags",
                  "mags_h", "mags_p"]
         nf = {"gas": 6, "gas_h": 6, "gas_p": 6}
-        out = {}
+        out = dict(out or {})
         args = []
         for nm in names:
             if nm in which:
-                out[nm] = np.zeros(self.shape(nf.get(nm, 3)))
+                shape = self.shape(nf.get(nm, 3))
+                if nm not in out:
+                    out[nm] = np.zeros(shape)
+                if out[nm].shape != shape or not out[nm].flags.c_contiguous or out[nm].dtype != np.float64:
+                    raise ValueError(f"{nm}: need a C-contiguous float64 array of shape {shape}")
                 args.append(_ptr(out[nm]))
             else:
                 args.append(None)
@@ -261,6 +267,20 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def problem_state(n, xs, kind, coord=COORD_CARTESIAN, **over):
+    """Host-only: initial (gas, face_b) arrays of a problem on a grid."""
+    n = tuple(int(v) for v in n)
+    N = tuple(v + 2 * NG + 1 for v in n)
+    xs = [np.ascontiguousarray(x, dtype=np.float64) for x in xs]
+    d = Desc(n[0], n[1], n[2], coord, _ptr(xs[0]), _ptr(xs[1]), _ptr(xs[2]), b"pppppp",
+             0, 0, 0, 0, 0, 0)
+    gas = np.zeros((6,) + N)
+    fb = np.zeros((3,) + N)
+    p = problem(kind, **over)
+    _check(lib().gop_problem_init(C.byref(d), C.byref(p), _ptr(gas), _ptr(fb)))
+    return gas, fb
 
 
 def make(kind, n, domain=None, coord=None, bc="pppppp", precision=PREC_FP64, **over):

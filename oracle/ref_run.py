@@ -82,6 +82,7 @@ class RefRun:
     wall_steps: int = 0
     wall_seconds: float = 0.0
     files: list = field(default_factory=list)
+    step_starts: list = field(default_factory=list)
 
     def state(self, idx: int = -1) -> dict:
         """Primitive state and face B (ghost-extended, reference layout
@@ -151,6 +152,10 @@ def run(
             calls = int(m.group(1))
             rr.wall_steps = calls - 2
             rr.wall_seconds = float(m.group(3)) - float(m.group(2))
+        m = re.search(r"GOP_SHIM_TIMES ([\d. ]+)", p.stderr)
+        if m:
+            # call 0 = initial dt, call n = start of step n
+            rr.step_starts = [float(v) for v in m.group(1).split()][1:]
         return rr
     finally:
         shutil.rmtree(tmp, ignore_errors=True)

@@ -44,9 +44,15 @@ int MPI_Finalize(void) {
    * initial dt (src/solver_solve.c:97), call n >= 1 opens step n
    * (src/solver_solve.c:105), so calls 1..last bracket last-1 whole steps. */
   const char *e = getenv("GOP_SHIM_TIMING");
-  if (e && e[0] == '1' && g_ntimes >= 3) {
+  if (e && (e[0] == '1' || e[0] == '2') && g_ntimes >= 3) {
     fprintf(stderr, "GOP_SHIM_TIMING calls=%d t1=%.9f tlast=%.9f\n", g_ntimes,
             g_times[1], g_times[g_ntimes - 1]);
+  }
+  /* GOP_SHIM_TIMING=2 also lists every timestamp (per-step durations) */
+  if (e && e[0] == '2') {
+    fprintf(stderr, "GOP_SHIM_TIMES");
+    for (int n = 0; n < g_ntimes; n++) fprintf(stderr, " %.9f", g_times[n]);
+    fprintf(stderr, "\n");
   }
   return MPI_SUCCESS;
 }
