@@ -273,6 +273,13 @@ int check_desc(const gop_desc* d) {
       return fail(GOP_EINVAL, "bad boundary kind on axis %d", a);
     if ((lo == 'p') != (hi == 'p'))
       return fail(GOP_EINVAL, "axis %d: periodic must be set on both faces", a);
+    for (int s = 0; s < 2; s++) {
+      char g = d->gem_bc[2 * a + s], b = d->bc[2 * a + s];
+      if (g == 0) continue;
+      if (!strchr("psrfen", g)) return fail(GOP_EINVAL, "bad face-field boundary kind on axis %d", a);
+      if ((g == 'p') != (b == 'p'))
+        return fail(GOP_EINVAL, "axis %d: gas and face field disagree on periodicity", a);
+    }
   }
   if (d->precision != GOP_PREC_FP64 && d->precision != GOP_PREC_MIXED)
     return fail(GOP_EINVAL, "precision must be GOP_PREC_FP64 or GOP_PREC_MIXED");
@@ -393,6 +400,8 @@ int gop_create(const gop_desc* desc, gop_instance** out) {
   if (!h) return fail(GOP_ENOMEM, "host allocation failed");
   h->d = *desc;
   gop_desc& d = h->d;
+  for (int f = 0; f < 6; f++)
+    if (d.gem_bc[f] == 0) d.gem_bc[f] = d.bc[f];
   if (d.gamma == 0) d.gamma = kGamma;
   if (d.cfl == 0) d.cfl = kCfl;
   if (d.ca == 0) d.ca = kCa;
@@ -526,7 +535,7 @@ int gop_prepare(gop_instance* h, int restart) {
   if (!h) return fail(GOP_EINVAL, "instance is NULL");
   const Params& P = h->P;
   // halo + boundary fill of the current state (src/solver_solve.c:25-40)
-  launch_ghosts(P, h->d.bc, 1, h->st);
+  launch_ghosts(P, h->d.bc, h->d.gem_bc, 1, h->st);
   if (!restart) {
     // AB2 history <- current state (src/solver_solve.c:55-92)
     CK(cudaMemcpyAsync(P.Wbuf[1], P.Wbuf[0], (size_t)P.fs * 6 * sizeof(double),
@@ -577,7 +586,7 @@ static int enqueue_steps(gop_instance* h, int nsteps, double time_stop) {
     else
       launch_step_body<double>(P, h->d.coord, h->wd, h->st, hook);
     hook(G_GHOST, 1);
-    launch_ghosts(P, h->d.bc, 0, h->st);
+    launch_ghosts(P, h->d.bc, h->d.gem_bc, 0, h->st);
     hook(G_GHOST, 0);
     hook(G_END, 1);
     launch_end(P, h->st);

@@ -631,9 +631,10 @@ __global__ void k_wrap(Params P, int axis, int which) {
   }
 }
 
-// One face of the ghost-fill library (src/boundary_conditions.c) for the 6
-// gas primitives and the 3 face fields.
-__global__ void k_bcface(Params P, int axis, int side, int kind, int which) {
+// One face of the ghost-fill library (src/boundary_conditions.c): the 6 gas
+// primitives with kind `kind` (gas_bc_*) and the 3 face fields with kind
+// `gkind` (gem_bc_*); 0 skips that group.
+__global__ void k_bcface(Params P, int axis, int side, int kind, int gkind, int which) {
   if (stopped(P)) return;
   const int bsel = which ? cur_buf(P) : 1 - cur_buf(P);
   double* __restrict__ W = P.Wbuf[bsel];
@@ -649,12 +650,14 @@ __global__ void k_bcface(Params P, int axis, int side, int kind, int which) {
   ijk[ob] = u;
   for (int f = 0; f < 9; f++) {
     bool gas = f < 6;
-    if (!gas && kind == 'r') continue;  // gem_bc_reflective_* are empty
+    int kd = gas ? kind : gkind;
+    if (kd == 0 || kd == 'n' || kd == 'p') continue;
+    if (!gas && kd == 'r') continue;  // gem_bc_reflective_* are empty
     int onface = (!gas && f - 6 == axis) ? 1 : 0;
     double* a = gas ? W + (size_t)f * P.fs : B + (size_t)(f - 6) * P.fs;
     int dst = side == 0 ? l : N - 1 - NGH + l + onface;
     double v;
-    if (kind == 'f') {
+    if (kd == 'f') {
       if (gas) {
         if (f == PS) continue;
         if (f == RHO) v = (axis == 1 && side == 0) ? 2.0 : 1.0;
@@ -665,11 +668,11 @@ __global__ void k_bcface(Params P, int axis, int side, int kind, int which) {
       }
     } else {
       int src;
-      if (kind == 'e') src = side == 0 ? NGH : N - 1 - NGH - 1 + onface;
+      if (kd == 'e') src = side == 0 ? NGH : N - 1 - NGH - 1 + onface;
       else src = side == 0 ? 2 * NGH - 1 - l + onface : N - 1 - NGH - 1 - l;
       ijk[axis] = src;
       v = a[lin(P, ijk[0], ijk[1], ijk[2])];
-      if (kind == 'r' && gas && f == V1 + axis) v = -v;
+      if (kd == 'r' && gas && f == V1 + axis) v = -v;
     }
     ijk[axis] = dst;
     a[lin(P, ijk[0], ijk[1], ijk[2])] = v;
@@ -790,7 +793,8 @@ template void launch_step_body<double>(const Params&, int, const Work<double>&, 
 template void launch_step_body<float>(const Params&, int, const Work<float>&, cudaStream_t,
                                       const Hook&);
 
-void launch_ghosts(const Params& P, const char bc[6], int which, cudaStream_t st) {
+void launch_ghosts(const Params& P, const char bc[6], const char gem_bc[6], int which,
+                   cudaStream_t st) {
   dim3 blk(32, 8, 1);
   bool periodic[3];
   for (int a = 0; a < 3; a++) periodic[a] = bc[2 * a] == 'p' && bc[2 * a + 1] == 'p';
@@ -804,11 +808,14 @@ void launch_ghosts(const Params& P, const char bc[6], int which, cudaStream_t st
   }
   for (int face = 0; face < 6; face++) {
     int a = face / 2, side = face % 2;
-    char kind = bc[face];
-    if (periodic[a] || kind == 'n' || kind == 'p') continue;
+    char kind = bc[face], gkind = gem_bc[face];
+    if (periodic[a]) continue;
+    bool gas_work = kind != 'n';
+    bool gem_work = gkind != 'n' && gkind != 'r';
+    if (!gas_work && !gem_work) continue;
     int oa = (a + 1) % 3, ob = (a + 2) % 3;
     dim3 g((P.N[oa] + blk.x - 1) / blk.x, (P.N[ob] + blk.y - 1) / blk.y, NGH);
-    LAUNCH(k_bcface, g, blk, st, P, a, side, (int)kind, which);
+    LAUNCH(k_bcface, g, blk, st, P, a, side, (int)kind, (int)gkind, which);
   }
 }
 

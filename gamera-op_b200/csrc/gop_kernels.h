@@ -42,7 +42,8 @@ template <typename R>
 void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t st,
                       const Hook& hook = Hook());
 // which = 0: the buffer being written this step; 1: the current state
-void launch_ghosts(const Params& P, const char bc[6], int which, cudaStream_t st);
+void launch_ghosts(const Params& P, const char bc[6], const char gem_bc[6], int which,
+                   cudaStream_t st);
 void launch_from_ref(const Params& P, int nf, const double* src, double* dst, cudaStream_t st);
 void launch_to_ref(const Params& P, int nf, const double* src, double* dst, cudaStream_t st);
 template <typename R>

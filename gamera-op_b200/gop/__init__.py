@@ -41,6 +41,7 @@ class Desc(C.Structure):
         ("ni", C.c_int), ("nj", C.c_int), ("nk", C.c_int), ("coord", C.c_int),
         ("x1", _dp), ("x2", _dp), ("x3", _dp),
         ("bc", C.c_char * 6),
+        ("gem_bc", C.c_char * 6),
         ("precision", C.c_int),
         ("gamma", C.c_double), ("cfl", C.c_double), ("ca", C.c_double),
         ("rho_floor", C.c_double), ("p_floor", C.c_double),
@@ -142,14 +143,15 @@ class Instance:
 
     def __init__(self, n, x1, x2, x3, coord=COORD_CARTESIAN, bc="pppppp",
                  precision=PREC_FP64, gamma=0.0, cfl=0.0, ca=0.0, rho_floor=0.0,
-                 p_floor=0.0):
+                 p_floor=0.0, gem_bc=""):
         self.n = tuple(int(v) for v in n)
         self.N = tuple(v + 2 * NG + 1 for v in self.n)
         self._x = [np.ascontiguousarray(x, dtype=np.float64) for x in (x1, x2, x3)]
         self.coord, self.bc, self.precision = coord, bc, precision
         self.desc = Desc(self.n[0], self.n[1], self.n[2], coord,
                          _ptr(self._x[0]), _ptr(self._x[1]), _ptr(self._x[2]),
-                         bc.encode(), precision, gamma, cfl, ca, rho_floor, p_floor)
+                         bc.encode(), gem_bc.encode(), precision, gamma, cfl, ca, rho_floor,
+                         p_floor)
         h = C.c_void_p()
         _check(lib().gop_create(C.byref(self.desc), C.byref(h)))
         self._h = h
@@ -275,7 +277,7 @@ def problem_state(n, xs, kind, coord=COORD_CARTESIAN, **over):
     N = tuple(v + 2 * NG + 1 for v in n)
     xs = [np.ascontiguousarray(x, dtype=np.float64) for x in xs]
     d = Desc(n[0], n[1], n[2], coord, _ptr(xs[0]), _ptr(xs[1]), _ptr(xs[2]), b"pppppp",
-             0, 0, 0, 0, 0, 0)
+             b"", 0, 0, 0, 0, 0, 0)
     gas = np.zeros((6,) + N)
     fb = np.zeros((3,) + N)
     p = problem(kind, **over)

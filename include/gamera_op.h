@@ -61,6 +61,8 @@ typedef struct {
   const double *x2;   /* nj+9 values, x2[0][j][0] */
   const double *x3;   /* nk+9 values, x3[0][0][k] */
   char bc[6];         /* faces i-lo,i-hi,j-lo,j-hi,k-lo,k-hi (GOP_BC_*) */
+  char gem_bc[6];     /* ghost fill of the face field per face; 0 = same as bc
+                         (gas_bc_* and gem_bc_* are separate hooks in the reference) */
   int precision;      /* GOP_PREC_* */
   /* physics constants of src/config.c:82-97 (0 selects the default) */
   double gamma;       /* 5/3 */

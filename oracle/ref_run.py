@@ -113,6 +113,8 @@ def run(
     keep_output: bool = True,
     time_stop: float = 1e30,
     timeout: float | None = None,
+    exe: str | os.PathLike | None = None,
+    output_interval: float = 1e30,
 ) -> RefRun:
     """Runs ``steps`` steps of the reference on an ``n=(ni,nj,nk)`` grid.
 
@@ -120,7 +122,7 @@ def run(
     otherwise writes are discarded (used for timing) and the shim reports the
     wall time of the step loop.
     """
-    exe = binary(coord, flavor)
+    exe = Path(exe) if exe else binary(coord, flavor)
     if not exe.exists():
         raise FileNotFoundError(f"{exe} is not built (make -C oracle reference)")
     ni, nj, nk = n
@@ -130,7 +132,7 @@ def run(
             f"ni_global: {ni}\nnj_global: {nj}\nnk_global: {nk}\n"
             "proc_dims_i: 1\nproc_dims_j: 1\nproc_dims_k: 1\n"
             f"Nt: {steps}\ntime_stop: {time_stop!r}\n"
-            "output_interval: 1e30\n"
+            f"output_interval: {output_interval!r}\n"
             "x_Norm: 1.0\nu_Norm: 1.0\nrho_Norm: 1.0\n"
         )
         Path(tmp, "config.yaml").write_text(cfg)

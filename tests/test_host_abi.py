@@ -34,7 +34,7 @@ def test_create_rejects_bad_descriptors_without_touching_the_device():
     x = gop.grid_uniform(8, 0.0, 1.0)
     bad = gop.Desc(2, 8, 8, 0, x.ctypes.data_as(C.POINTER(C.c_double)),
                    x.ctypes.data_as(C.POINTER(C.c_double)),
-                   x.ctypes.data_as(C.POINTER(C.c_double)), b"pppppp", 0, 0, 0, 0, 0, 0)
+                   x.ctypes.data_as(C.POINTER(C.c_double)), b"pppppp", b"", 0, 0, 0, 0, 0, 0)
     h = C.c_void_p()
     assert gop.lib().gop_create(C.byref(bad), C.byref(h)) == -22
     assert b"at least" in gop.lib().gop_last_error()
@@ -60,7 +60,7 @@ def _host_init(name, kind, **over):
     xs = [np.ascontiguousarray(g[f"x{a + 1}"]) for a in range(3)]
     N = tuple(v + 9 for v in n)
     d = gop.Desc(n[0], n[1], n[2], coord, *(x.ctypes.data_as(C.POINTER(C.c_double)) for x in xs),
-                 str(g["bc"]).encode(), 0, 0, 0, 0, 0, 0)
+                 str(g["bc"]).encode(), b"", 0, 0, 0, 0, 0, 0)
     p = gop.problem(kind, **over)
     gas = np.zeros((6,) + N)
     fb = np.zeros((3,) + N)
