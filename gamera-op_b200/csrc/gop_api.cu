@@ -14,6 +14,7 @@
 
 #include "gamera_op.h"
 #include "gop_device.cuh"
+#include "gop_internal.h"
 #include "gop_kernels.h"
 
 using namespace gop;
@@ -258,7 +259,17 @@ void build_tables(const gop_desc& d, Tables& T) {
   }
 }
 
-int check_desc(const gop_desc* d) {
+}  // namespace
+
+int gop::set_error(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+int gop::check_desc(const gop_desc* d) {
   if (!d) return fail(GOP_EINVAL, "desc is NULL");
   if (d->ni < NGH || d->nj < NGH || d->nk < NGH)
     return fail(GOP_EINVAL, "each axis needs at least %d active cells", NGH);
@@ -285,6 +296,8 @@ int check_desc(const gop_desc* d) {
     return fail(GOP_EINVAL, "precision must be GOP_PREC_FP64 or GOP_PREC_MIXED");
   return GOP_OK;
 }
+
+namespace {
 
 struct Layout {
   int N[3];

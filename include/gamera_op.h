@@ -143,6 +143,31 @@ const char *gop_last_error(void);
 /* Kernels launched by this library since load (for launch accounting). */
 int64_t gop_kernel_launches(void);
 
+/* ---- CFL dt of a caller-owned device state, allocating nothing -------- */
+
+/* No counterpart in the reference: GAMERA-OP has no GPU and no allocation
+ * constraints.  This is the one entry point for callers that must not
+ * allocate device memory -- e.g. code between the capture calls of a CUDA
+ * graph, where cudaMalloc is not capturable, or a serving loop whose device
+ * memory was reserved at start-up and may not grow.
+ *
+ * gas (6 fields) and face_b (3 fields) are DEVICE pointers in the layout of
+ * gop_upload; out is a device pointer to 2 doubles that receives the CFL dt
+ * (get_dt_normal, src/solver_func.c:255-298) and max|div B|
+ * (src/solver_func.c:324-343) over the active cells.  Asynchronous on
+ * `stream` (cudaStream_t as void*); it calls no cudaMalloc/cudaFree.
+ *
+ * Its scratch is one file-scope device array of GOP_NOALLOC_SCRATCH_DOUBLES
+ * doubles (64 KiB), held by every GPU that loads the library until exit, so
+ * grids are limited to GOP_NOALLOC_MAX_N active cells per axis (larger ones
+ * are rejected with GOP_EINVAL).  The first call on a device looks up that
+ * array's device address; make it before any stream capture.  All calls
+ * share the array: calls whose kernels overlap on the GPU race. */
+#define GOP_NOALLOC_MAX_N 1024
+#define GOP_NOALLOC_SCRATCH_DOUBLES 8192
+int gop_cfl_dt_noalloc(const gop_desc *desc, const double *gas, const double *face_b,
+                       double *out, void *stream);
+
 /* ---- host-only problem setup (no device work) ------------------------ */
 
 /* Face coordinates of the reference's default uniform grid
