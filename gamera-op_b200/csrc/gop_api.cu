@@ -443,6 +443,8 @@ int gop_create(const gop_desc* desc, gop_instance** out) {
   P.p_floor = d.p_floor;
   P.pdm_a1 = kPdmb / (kPdmb + 1.0);
   P.pdm_a2 = 1.0 - P.pdm_a1;
+  P.inv_gm1 = 1.0 / P.gm1;
+  P.q_ca = 0.25 / d.ca;
 
   size_t rsize = d.precision == GOP_PREC_MIXED ? sizeof(float) : sizeof(double);
   size_t ref = (size_t)L.N[0] * L.N[1] * L.N[2];

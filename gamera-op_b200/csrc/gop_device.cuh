@@ -68,6 +68,8 @@ struct Params {
   int tmax;
   double gamma, gm1, cfl, ca, ca2, rho_floor, p_floor;
   double pdm_a1, pdm_a2;  // PDMB/(PDMB+1), 1-a1
+  double inv_gm1;         // 1/(gamma-1)
+  double q_ca;            // 1/(4 CA): Boris diffusion coefficient of the stress
   double* scal;           // device scalars
   double* Wbuf[2];        // two 6-field primitive buffers (current / next)
   double* Bbuf[2];        // two 3-field face-B buffers

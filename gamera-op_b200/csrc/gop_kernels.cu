@@ -213,203 +213,204 @@ __global__ void k_ab2(Params P, Work<R> w) {
 
 // ------------------------------------------------------------- edge EMF
 
-// load v[0..7] = field at cells f-4..f+3 along axis s from x (x at cell f)
-template <typename R, typename T>
-__device__ __forceinline__ void line8(const T* __restrict__ a, long long x, long long s, R v[8]) {
-#pragma unroll
-  for (int t = 0; t < 8; t++) v[t] = (R)a[x + (t - 4) * s];
+template <int AX>
+__device__ __forceinline__ long long sd(const Params& P) {
+  return AX == 0 ? 1LL : (AX == 1 ? P.sj : P.sk);
 }
 
+// v[0..7] = a[(t-4)*s]: cells f-4..f+3 along stride s, a pointing at cell f
+template <typename R, typename T>
+__device__ __forceinline__ void line8(const T* __restrict__ a, long long s, R v[8]) {
+#pragma unroll
+  for (int t = 0; t < 8; t++) v[t] = (R)a[(t - 4) * s];
+}
+
+__device__ __forceinline__ double rsq(double x) { return rsqrt(x); }
+__device__ __forceinline__ float rsq(float x) { return rsqrtf(x); }
+
 // First centre-to-edge sweep of center2corner_{jk,ki,ij}
-// (src/solver_func.c:686-778): for edge direction d, velocity components
-// p=(d+1)%3 and q=(d+2)%3 reconstructed along p (limiter on the step-start
-// velocity) and averaged.  Points: d active, p faces lo..hi+1, q all ghosts.
-template <typename R>
-__global__ void k_c2c(Params P, int d, Work<R> wk) {
+// (src/solver_func.c:686-778): for edges along D, velocity components
+// p=(D+1)%3 and q=(D+2)%3 reconstructed along p (limiter on the step-start
+// velocity) and averaged.  Points: D active, p faces lo..hi+1, q all ghosts.
+template <typename R, int D>
+__global__ void __launch_bounds__(256) k_c2c(Params P, Work<R> wk) {
+  constexpr int p = (D + 1) % 3, q = (D + 2) % 3;
   if (stopped(P)) return;
-  const double* __restrict__ W = P.Wbuf[cur_buf(P)];
-  const R* __restrict__ Wh = wk.Wh;
-  R* __restrict__ Vint = wk.V;
-  int p = (d + 1) % 3, q = (d + 2) % 3;
-  int t0 = blockIdx.x * blockDim.x + threadIdx.x;
-  int t1 = blockIdx.y * blockDim.y + threadIdx.y;
-  int t2 = blockIdx.z * blockDim.z + threadIdx.z;
-  int ijk[3] = {t0, t1, t2};
-  // ranges: axis d [NGH, NGH+n-1], axis p [NGH, NGH+n], axis q [0, n+2*NGH-1]
-  int lo[3], cnt[3];
-  lo[d] = NGH; cnt[d] = P.n[d];
+  int ijk[3] = {(int)(blockIdx.x * blockDim.x + threadIdx.x),
+                (int)(blockIdx.y * blockDim.y + threadIdx.y),
+                (int)(blockIdx.z * blockDim.z + threadIdx.z)};
+  int cnt[3], lo[3];
+  lo[D] = NGH; cnt[D] = P.n[D];
   lo[p] = NGH; cnt[p] = P.n[p] + 1;
   lo[q] = 0;   cnt[q] = P.n[q] + 2 * NGH;
   if (ijk[0] >= cnt[0] || ijk[1] >= cnt[1] || ijk[2] >= cnt[2]) return;
   int i = ijk[0] + lo[0], j = ijk[1] + lo[1], k = ijk[2] + lo[2];
-  int f = p == 0 ? i : (p == 1 ? j : k);
-  long long x = lin(P, i, j, k), s = stride(P, p);
+  const int f = p == 0 ? i : (p == 1 ? j : k);
+  const long long x = lin(P, i, j, k), s = sd<p>(P);
+  const size_t fs = P.fs;
+  const double* __restrict__ W = P.Wbuf[cur_buf(P)] + x;
   FaceWeights<R> Wt;
   load_weights<R>(P, p, f, Wt);
   const R a1 = (R)P.pdm_a1, a2 = (R)P.pdm_a2;
 #pragma unroll
   for (int cc = 0; cc < 2; cc++) {
-    int comp = cc == 0 ? p : q;
+    const int comp = cc == 0 ? p : q;
     R v[8], lim[4], L, Rr;
-    line8<R, R>(Wh + (size_t)(V1 + comp) * P.fs, x, s, v);
+    line8<R, R>(wk.Wh + (size_t)(V1 + comp) * fs + x, s, v);
 #pragma unroll
-    for (int t = 0; t < 4; t++) lim[t] = (R)W[x + (V1 + comp) * P.fs + (t - 2) * s];
+    for (int t = 0; t < 4; t++) lim[t] = (R)W[(V1 + comp) * fs + (t - 2) * s];
     recon_lr<R>(v, lim, Wt, a1, a2, L, Rr);
-    Vint[x + (size_t)(2 * d + cc) * P.fs] = R(0.5) * (L + Rr);
+    wk.V[x + (size_t)(2 * D + cc) * fs] = R(0.5) * (L + Rr);
   }
 }
 
 // Second sweep, face-field reconstruction and the edge EMF
-// (src/solver_func.c:779-902) for edges along d: d active, p and q faces.
-template <typename R>
-__global__ void k_emf(Params P, int d, Work<R> wk) {
+// (src/solver_func.c:779-902) for edges along D: D active, p and q faces.
+template <typename R, int D>
+__global__ void __launch_bounds__(256) k_emf(Params P, Work<R> wk) {
+  constexpr int p = (D + 1) % 3, q = (D + 2) % 3;
   if (stopped(P)) return;
-  const double* __restrict__ B = P.Bbuf[cur_buf(P)];
-  const R* __restrict__ Bh = wk.Bh;
-  const R* __restrict__ Wh = wk.Wh;
-  const R* __restrict__ Vint = wk.V;
-  R* __restrict__ E = wk.E;
-  int p = (d + 1) % 3, q = (d + 2) % 3;
   int ijk[3] = {(int)(blockIdx.x * blockDim.x + threadIdx.x),
                 (int)(blockIdx.y * blockDim.y + threadIdx.y),
                 (int)(blockIdx.z * blockDim.z + threadIdx.z)};
   int cnt[3];
-  cnt[d] = P.n[d];
+  cnt[D] = P.n[D];
   cnt[p] = P.n[p] + 1;
   cnt[q] = P.n[q] + 1;
   if (ijk[0] >= cnt[0] || ijk[1] >= cnt[1] || ijk[2] >= cnt[2]) return;
-  int i = ijk[0] + NGH, j = ijk[1] + NGH, k = ijk[2] + NGH;
-  int pos[3] = {i, j, k};
-  long long x = lin(P, i, j, k), sp = stride(P, p), sq = stride(P, q);
+  const int i = ijk[0] + NGH, j = ijk[1] + NGH, k = ijk[2] + NGH;
+  const int pos[3] = {i, j, k};
+  const long long x = lin(P, i, j, k), sp = sd<p>(P), sq = sd<q>(P);
+  const size_t fs = P.fs;
+  const double* __restrict__ B = P.Bbuf[cur_buf(P)] + x;
   const R a1 = (R)P.pdm_a1, a2 = (R)P.pdm_a2;
-  R vav[2];
+  R vav[2], bpl, bpr, bql, bqr;
   {
     FaceWeights<R> Wt;
     load_weights<R>(P, q, pos[q], Wt);
 #pragma unroll
     for (int cc = 0; cc < 2; cc++) {
       R v[8], lim[4], L, Rr;
-      line8<R, R>(Vint + (size_t)(2 * d + cc) * P.fs, x, sq, v);
+      line8<R, R>(wk.V + (size_t)(2 * D + cc) * fs + x, sq, v);
 #pragma unroll
       for (int t = 0; t < 4; t++) lim[t] = v[t + 2];
       recon_lr<R>(v, lim, Wt, a1, a2, L, Rr);
       vav[cc] = R(0.5) * (L + Rr);
     }
-  }
-  // B_p along q and B_q along p
-  R bpl, bpr, bql, bqr;
-  {
-    FaceWeights<R> Wt;
-    load_weights<R>(P, q, pos[q], Wt);
+    // B_p along q
     R v[8], lim[4];
-    line8<R, R>(Bh + (size_t)p * P.fs, x, sq, v);
+    line8<R, R>(wk.Bh + (size_t)p * fs + x, sq, v);
 #pragma unroll
-    for (int t = 0; t < 4; t++) lim[t] = (R)B[x + p * P.fs + (t - 2) * sq];
+    for (int t = 0; t < 4; t++) lim[t] = (R)B[p * fs + (t - 2) * sq];
     recon_lr<R>(v, lim, Wt, a1, a2, bpl, bpr);
   }
   {
+    // B_q along p
     FaceWeights<R> Wt;
     load_weights<R>(P, p, pos[p], Wt);
     R v[8], lim[4];
-    line8<R, R>(Bh + (size_t)q * P.fs, x, sp, v);
+    line8<R, R>(wk.Bh + (size_t)q * fs + x, sp, v);
 #pragma unroll
-    for (int t = 0; t < 4; t++) lim[t] = (R)B[x + q * P.fs + (t - 2) * sp];
+    for (int t = 0; t < 4; t++) lim[t] = (R)B[q * fs + (t - 2) * sp];
     recon_lr<R>(v, lim, Wt, a1, a2, bql, bqr);
   }
-  R bp = R(0.5) * (bpl + bpr), bq = R(0.5) * (bql + bqr);
-  R vp = vav[0], vq = vav[1];
+  const R bp = R(0.5) * (bpl + bpr), bq = R(0.5) * (bql + bqr);
+  const R vp = vav[0], vq = vav[1];
   R e = -(vp * bq - vq * bp);
-  const R* rh = Wh;  // density slot
-  R rho4 = rh[x - sp - sq] + rh[x - sp] + rh[x - sq] + rh[x];
-  if (d == 1) rho4 = rh[x - sq - sp] + rh[x - sq] + rh[x - sp] + rh[x];
-  R ca = (R)P.ca;
+  const R* rh = wk.Wh + x;  // density slot
+  // the reference sums the four densities around the edge in (i,j,k) order
+  R rho4 = D == 1 ? rh[-sq - sp] + rh[-sq] + rh[-sp] + rh[0]
+                  : rh[-sp - sq] + rh[-sp] + rh[-sq] + rh[0];
+  const R ca = (R)P.ca;
   R vz = sqrt((bp * bp + bq * bq) / (R(0.25) * rho4));
-  vz = vz * ca / sqrt(vz * vz + ca * ca) + sqrt(vp * vp + vq * vq);
+  vz = vz * ca * rsq(vz * vz + ca * ca) + sqrt(vp * vp + vq * vq);
   e += R(0.5) * vz * (bpl + bqr - bpr - bql);
-  E[x + (size_t)d * P.fs] = e;
+  wk.E[x + (size_t)D * fs] = e;
 }
 
 // ------------------------------------------------------------ face flux
 
-// Rusanov hydro flux and Maxwell stress at faces normal to d
+// Rusanov hydro flux and Maxwell stress at faces normal to D
 // (src/solver_func.c:934-1529).  F[9] = mass, 3 momenta, energy, entropy,
 // 3 stress components.
-template <typename R>
-__global__ void k_flux(Params P, int d, Work<R> wk) {
+template <typename R, int D>
+__global__ void __launch_bounds__(256, 2) k_flux(Params P, Work<R> wk) {
   if (stopped(P)) return;
-  const double* __restrict__ W = P.Wbuf[cur_buf(P)];
-  const double* __restrict__ B = P.Bbuf[cur_buf(P)];
-  const R* __restrict__ Wh = wk.Wh;
-  const R* __restrict__ Ms = wk.Ms;
-  const R* __restrict__ Msh = wk.Msh;
-  R* __restrict__ F = wk.F;
-  int ijk[3] = {(int)(blockIdx.x * blockDim.x + threadIdx.x),
-                (int)(blockIdx.y * blockDim.y + threadIdx.y),
-                (int)(blockIdx.z * blockDim.z + threadIdx.z)};
-  int cnt[3] = {P.n[0], P.n[1], P.n[2]};
-  cnt[d] += 1;
-  if (ijk[0] >= cnt[0] || ijk[1] >= cnt[1] || ijk[2] >= cnt[2]) return;
-  int i = ijk[0] + NGH, j = ijk[1] + NGH, k = ijk[2] + NGH;
-  int f = d == 0 ? i : (d == 1 ? j : k);
-  long long x = lin(P, i, j, k), s = stride(P, d);
+  const int i = NGH + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = NGH + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = NGH + blockIdx.z * blockDim.z + threadIdx.z;
+  if (i >= NGH + P.n[0] + (D == 0) || j >= NGH + P.n[1] + (D == 1) ||
+      k >= NGH + P.n[2] + (D == 2))
+    return;
+  const int f = D == 0 ? i : (D == 1 ? j : k);
+  const long long x = lin(P, i, j, k), s = sd<D>(P);
+  const size_t fs = P.fs;
+  const int cb = cur_buf(P);
+  const double* __restrict__ W = P.Wbuf[cb] + x;
   FaceWeights<R> Wt;
-  load_weights<R>(P, d, f, Wt);
+  load_weights<R>(P, D, f, Wt);
   const R a1 = (R)P.pdm_a1, a2 = (R)P.pdm_a2;
   R L[6], Rt[6], mL[3], mR[3];
 #pragma unroll
   for (int m = 0; m < 6; m++) {
     R v[8], lim[4];
-    line8<R, R>(Wh + (size_t)m * P.fs, x, s, v);
+    line8<R, R>(wk.Wh + (size_t)m * fs + x, s, v);
 #pragma unroll
-    for (int t = 0; t < 4; t++) lim[t] = (R)W[x + m * P.fs + (t - 2) * s];
+    for (int t = 0; t < 4; t++) lim[t] = (R)W[m * fs + (t - 2) * s];
     recon_lr<R>(v, lim, Wt, a1, a2, L[m], Rt[m]);
   }
 #pragma unroll
   for (int a = 0; a < 3; a++) {
     R v[8], lim[4];
-    line8<R, R>(Msh + (size_t)a * P.fs, x, s, v);
+    line8<R, R>(wk.Msh + (size_t)a * fs + x, s, v);
+    const R* ms = wk.Ms + (size_t)a * fs + x;
 #pragma unroll
-    for (int t = 0; t < 4; t++) lim[t] = Ms[x + a * P.fs + (t - 2) * s];
+    for (int t = 0; t < 4; t++) lim[t] = ms[(t - 2) * s];
     recon_lr<R>(v, lim, Wt, a1, a2, mL[a], mR[a]);
   }
-  const R gm = (R)P.gamma, gm1 = (R)P.gm1, ca = (R)P.ca;
-  R rl = L[RHO], rr = Rt[RHO], pl = L[PR], pr = Rt[PR], sl = L[PS], sr = Rt[PS];
-  R csl = sqrt(gm * pl / rl), csr = sqrt(gm * pr / rr);
-  R csel = sqrt(gm * sl / rl), cser = sqrt(gm * sr / rr);
-  R btl = mL[0] * mL[0] + mL[1] * mL[1] + mL[2] * mL[2];
-  R btr = mR[0] * mR[0] + mR[1] * mR[1] + mR[2] * mR[2];
-  R val = sqrt(btl / rl), var = sqrt(btr / rr);
-  R vel = val * ca / sqrt(val * val + ca * ca);
-  R ver = var * ca / sqrt(var * var + ca * ca);
-  R vnl = L[V1 + d], vnr = Rt[V1 + d];
-  R vf = fmax(fabs(vnl) + sqrt(csl * csl + vel * vel), fabs(vnr) + sqrt(csr * csr + ver * ver));
-  R vfe = fmax(fabs(vnl) + sqrt(csel * csel + vel * vel), fabs(vnr) + sqrt(cser * cser + ver * ver));
+  const R gm = (R)P.gamma, gm1 = (R)P.gm1, ca = (R)P.ca, ca2 = (R)P.ca2;
+  const R rl = L[RHO], rr = Rt[RHO], pl = L[PR], pr = Rt[PR], sl = L[PS], sr = Rt[PS];
+  const R irl = R(1) / rl, irr = R(1) / rr;
+  const R csl = sqrt(gm * pl * irl), csr = sqrt(gm * pr * irr);
+  // entropy channel: p_S = 0 everywhere unless a problem sets it; the
+  // zero test only skips exact zeros
+  const R csel = sl == R(0) ? R(0) : sqrt(gm * sl * irl);
+  const R cser = sr == R(0) ? R(0) : sqrt(gm * sr * irr);
+  const R btl = mL[0] * mL[0] + mL[1] * mL[1] + mL[2] * mL[2];
+  const R btr = mR[0] * mR[0] + mR[1] * mR[1] + mR[2] * mR[2];
+  const R val = sqrt(btl * irl), var = sqrt(btr * irr);
+  const R vel = val * ca * rsq(val * val + ca2);
+  const R ver = var * ca * rsq(var * var + ca2);
+  const R vnl = L[V1 + D], vnr = Rt[V1 + D];
+  const R vf = fmax(fabs(vnl) + sqrt(csl * csl + vel * vel), fabs(vnr) + sqrt(csr * csr + ver * ver));
+  const R vfe = fmax(fabs(vnl) + sqrt(csel * csel + vel * vel), fabs(vnr) + sqrt(cser * cser + ver * ver));
   R mol[3], mor[3];
 #pragma unroll
   for (int a = 0; a < 3; a++) {
     mol[a] = rl * L[V1 + a];
     mor[a] = rr * Rt[V1 + a];
   }
-  R el = R(0.5) * rl * (L[V1] * L[V1] + L[V2] * L[V2] + L[V3] * L[V3]) + pl / gm1;
-  R er = R(0.5) * rr * (Rt[V1] * Rt[V1] + Rt[V2] * Rt[V2] + Rt[V3] * Rt[V3]) + pr / gm1;
-  R Sl = sl / pow(rl, gm1), Sr = sr / pow(rr, gm1);
-  const size_t fs = P.fs;
-  R* o = F + (size_t)(9 * d) * fs + x;
-  o[0] = R(0.5) * (mol[d] + mor[d] - vf * (rr - rl));
+  const R igm1 = (R)P.inv_gm1;
+  const R el = R(0.5) * rl * (L[V1] * L[V1] + L[V2] * L[V2] + L[V3] * L[V3]) + pl * igm1;
+  const R er = R(0.5) * rr * (Rt[V1] * Rt[V1] + Rt[V2] * Rt[V2] + Rt[V3] * Rt[V3]) + pr * igm1;
+  const R Sl = (sl == R(0) && rl > R(0)) ? sl : sl / pow(rl, gm1);
+  const R Sr = (sr == R(0) && rr > R(0)) ? sr : sr / pow(rr, gm1);
+  R* o = wk.F + (size_t)(9 * D) * fs + x;
+  o[0] = R(0.5) * (mol[D] + mor[D] - vf * (rr - rl));
 #pragma unroll
   for (int a = 0; a < 3; a++) {
     R t = mol[a] * vnl + mor[a] * vnr - vf * (mor[a] - mol[a]);
-    if (a == d) t = mol[a] * vnl + pl + mor[a] * vnr + pr - vf * (mor[a] - mol[a]);
+    if (a == D) t = mol[a] * vnl + pl + mor[a] * vnr + pr - vf * (mor[a] - mol[a]);
     o[(1 + a) * fs] = R(0.5) * t;
   }
   o[4 * fs] = R(0.5) * (el * vnl + pl * vnl + er * vnr + pr * vnr - vf * (er - el));
   o[5 * fs] = R(0.5) * (Sl * vnl + Sr * vnr - vfe * (Sr - Sl));
-  R bn = (R)B[x + d * fs];
-  R bq = (btl + btr) / R(4) / ca;
+  const R bn = (R)P.Bbuf[cb][x + D * fs];
+  const R bq = (btl + btr) * (R)P.q_ca;
 #pragma unroll
   for (int a = 0; a < 3; a++) {
     R tl, tr;
-    if (a == d) {
+    if (a == D) {
       tl = R(0.5) * (R(0.5) * btl - mL[a] * bn);
       tr = R(0.5) * (R(0.5) * btr - mR[a] * bn);
     } else {
@@ -422,112 +423,116 @@ __global__ void k_flux(Params P, int d, Work<R> wk) {
 
 // --------------------------------------------------------------- update
 
-// new face field of component a at face (i,j,k) by constrained transport
+// new face field of component A at face (i,j,k) by constrained transport
 // (src/solver_solve.c:263-306)
-template <int COORD, typename R>
+template <int COORD, int A, typename R>
 __device__ __forceinline__ double ct_face(const Params& P, const double* __restrict__ B,
-                                          const R* __restrict__ E, int a, int i, int j, int k,
+                                          const R* __restrict__ E, int i, int j, int k,
                                           double dt) {
-  int p = (a + 1) % 3, q = (a + 2) % 3;
-  long long x = lin(P, i, j, k), sp = stride(P, p), sq = stride(P, q);
-  int ip = i + (p == 0), jp = j + (p == 1), kp = k + (p == 2);
-  int iq = i + (q == 0), jq = j + (q == 1), kq = k + (q == 2);
+  constexpr int p = (A + 1) % 3, q = (A + 2) % 3;
+  const long long x = lin(P, i, j, k), sp = sd<p>(P), sq = sd<q>(P);
+  const int ip = i + (p == 0), jp = j + (p == 1), kp = k + (p == 2);
+  const int iq = i + (q == 0), jq = j + (q == 1), kq = k + (q == 2);
   const size_t fs = P.fs;
-  double cq = (double)E[x + sp + q * fs] * Geo<COORD>::edge(P, q, ip, jp, kp) -
-              (double)E[x + q * fs] * Geo<COORD>::edge(P, q, i, j, k);
-  double cp = (double)E[x + sq + p * fs] * Geo<COORD>::edge(P, p, iq, jq, kq) -
-              (double)E[x + p * fs] * Geo<COORD>::edge(P, p, i, j, k);
-  return B[x + a * fs] - dt * (cq - cp) / Geo<COORD>::face(P, a, i, j, k);
+  const double cq = (double)E[x + sp + q * fs] * Geo<COORD>::edge(P, q, ip, jp, kp) -
+                    (double)E[x + q * fs] * Geo<COORD>::edge(P, q, i, j, k);
+  const double cp = (double)E[x + sq + p * fs] * Geo<COORD>::edge(P, p, iq, jq, kq) -
+                    (double)E[x + p * fs] * Geo<COORD>::edge(P, p, i, j, k);
+  return B[x + A * fs] - dt * (cq - cp) / Geo<COORD>::face(P, A, i, j, k);
 }
 
 template <int COORD, typename R>
-__global__ void k_update(Params P, Work<R> wk) {
+__global__ void __launch_bounds__(256) k_update(Params P, Work<R> wk) {
   if (stopped(P)) return;
-  const int cb = cur_buf(P);
-  const double* __restrict__ W = P.Wbuf[cb];
-  const double* __restrict__ B = P.Bbuf[cb];
-  double* __restrict__ Wn = P.Wbuf[1 - cb];
-  double* __restrict__ Bn = P.Bbuf[1 - cb];
-  const R* __restrict__ Wh = wk.Wh;
-  const R* __restrict__ Msh = wk.Msh;
-  const R* __restrict__ F = wk.F;
-  const R* __restrict__ E = wk.E;
-  int i = NGH + blockIdx.x * blockDim.x + threadIdx.x;
-  int j = NGH + blockIdx.y * blockDim.y + threadIdx.y;
-  int k = NGH + blockIdx.z * blockDim.z + threadIdx.z;
+  const int i = NGH + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = NGH + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = NGH + blockIdx.z * blockDim.z + threadIdx.z;
   double dtc = DBL_MAX, dbmax = 0.0;
-  bool inside = i < NGH + P.n[0] && j < NGH + P.n[1] && k < NGH + P.n[2];
+  const bool inside = i < NGH + P.n[0] && j < NGH + P.n[1] && k < NGH + P.n[2];
   if (inside) {
     const size_t fs = P.fs;
     const double dt = P.scal[S_DT];
-    long long x = lin(P, i, j, k);
+    const int cb = cur_buf(P);
+    const double* __restrict__ W = P.Wbuf[cb];
+    const double* __restrict__ B = P.Bbuf[cb];
+    double* __restrict__ Wn = P.Wbuf[1 - cb];
+    double* __restrict__ Bn = P.Bbuf[1 - cb];
+    const R* __restrict__ F = wk.F;
+    const R* __restrict__ E = wk.E;
+    const long long x = lin(P, i, j, k);
     const double vol = Geo<COORD>::vol(P, i, j, k);
-    double du[6], dm[3];
+    const double ivol = 1.0 / vol;
+    double du[6], dm[3], fl[3], fu[3];
 #pragma unroll
     for (int d = 0; d < 3; d++) {
-      long long s = stride(P, d);
-      int i1 = i + (d == 0), j1 = j + (d == 1), k1 = k + (d == 2);
-      double f0 = Geo<COORD>::face(P, d, i, j, k), f1 = Geo<COORD>::face(P, d, i1, j1, k1);
-      const R* Fd = F + (size_t)(9 * d) * fs;
+      const long long s = stride(P, d);
+      const int i1 = i + (d == 0), j1 = j + (d == 1), k1 = k + (d == 2);
+      fl[d] = Geo<COORD>::face(P, d, i, j, k);
+      fu[d] = Geo<COORD>::face(P, d, i1, j1, k1);
+      const R* Fd = F + (size_t)(9 * d) * fs + x;
 #pragma unroll
       for (int m = 0; m < 6; m++) {
-        double v = ((double)Fd[x + s + m * fs] * f1 - (double)Fd[x + m * fs] * f0) / vol;
+        double v = ((double)Fd[s + m * fs] * fu[d] - (double)Fd[m * fs] * fl[d]) * ivol;
         du[m] = d == 0 ? v : du[m] + v;
       }
 #pragma unroll
       for (int a = 0; a < 3; a++) {
-        double v = ((double)Fd[x + s + (6 + a) * fs] * f1 - (double)Fd[x + (6 + a) * fs] * f0) / vol;
+        double v = ((double)Fd[s + (6 + a) * fs] * fu[d] - (double)Fd[(6 + a) * fs] * fl[d]) * ivol;
         dm[a] = d == 0 ? v : dm[a] + v;
       }
     }
     // spherical geometric sources (src/spherical/spherical_general.c:605-681)
     double sh[3] = {0.0, 0.0, 0.0}, sb[3] = {0.0, 0.0, 0.0};
     if (COORD == 2) {
-      long long si = 1, sjj = P.sj;
-      double fi0 = Geo<COORD>::face(P, 0, i, j, k), fi1 = Geo<COORD>::face(P, 0, i + 1, j, k);
-      double fj0 = Geo<COORD>::face(P, 1, i, j, k), fj1 = Geo<COORD>::face(P, 1, i, j + 1, k);
-      double dr = tb(P, 0, T_DX, i), rc = tb(P, 0, T_G3, i);
-      double ph = Wh[x + PR * fs], rh = Wh[x + RHO * fs], v2h = Wh[x + V2 * fs], v3h = Wh[x + V3 * fs];
-      double m22 = ph + rh * v2h * v2h, m33 = ph + rh * v3h * v3h;
-      const R* Fi = F;
-      const R* Fj = F + (size_t)9 * fs;
-      sh[0] = 0.5 * (m22 + m33) * (fi1 - fi0) / vol;
-      double s21 = -((double)Fi[x + 2 * fs] * fi0 + (double)Fi[x + si + 2 * fs] * fi1) * dr / rc / 2.0 / vol;
-      sh[1] = s21 + (fj1 - fj0) / vol * m33;
-      sh[2] = -((double)Fi[x + 3 * fs] * fi0 + (double)Fi[x + si + 3 * fs] * fi1) * dr / rc / 2.0 / vol;
-      double sd = tb(P, 1, T_G3, j), ss = tb(P, 1, T_G4, j);
-      sh[2] += -((double)Fj[x + 3 * fs] * fj0 + (double)Fj[x + sjj + 3 * fs] * fj1) * sd / ss / vol;
-      double b1 = Msh[x], b2 = Msh[x + fs], b3 = Msh[x + 2 * fs];
-      double bsq = b1 * b1 + b2 * b2 + b3 * b3;
-      double n22 = 0.5 * bsq - b2 * b2, n33 = 0.5 * bsq - b3 * b3;
-      sb[0] = 0.5 * (n22 + n33) * (fi1 - fi0) / vol;
-      double t21 = -((double)Fi[x + 7 * fs] * fi0 + (double)Fi[x + si + 7 * fs] * fi1) * dr / rc / 2.0 / vol;
-      sb[1] = t21 + (fj1 - fj0) / vol * n33;
-      sb[2] = -((double)Fi[x + 8 * fs] * fi0 + (double)Fi[x + si + 8 * fs] * fi1) * dr / rc / 2.0 / vol;
-      sb[2] += -((double)Fj[x + 8 * fs] * fj0 + (double)Fj[x + sjj + 8 * fs] * fj1) * sd / ss / vol;
+      const long long si = 1, sjj = P.sj;
+      const double fi0 = fl[0], fi1 = fu[0], fj0 = fl[1], fj1 = fu[1];
+      const double dr = tb(P, 0, T_DX, i), rc = tb(P, 0, T_G3, i);
+      const R* Wh = wk.Wh + x;
+      const double ph = Wh[PR * fs], rh = Wh[RHO * fs], v2h = Wh[V2 * fs], v3h = Wh[V3 * fs];
+      const double m22 = ph + rh * v2h * v2h, m33 = ph + rh * v3h * v3h;
+      const R* Fi = F + x;
+      const R* Fj = F + (size_t)9 * fs + x;
+      const double geo = dr / rc / 2.0 * ivol;
+      sh[0] = 0.5 * (m22 + m33) * (fi1 - fi0) * ivol;
+      sh[1] = -((double)Fi[2 * fs] * fi0 + (double)Fi[si + 2 * fs] * fi1) * geo + (fj1 - fj0) * ivol * m33;
+      sh[2] = -((double)Fi[3 * fs] * fi0 + (double)Fi[si + 3 * fs] * fi1) * geo;
+      const double sr = tb(P, 1, T_G3, j) / tb(P, 1, T_G4, j) * ivol;
+      sh[2] += -((double)Fj[3 * fs] * fj0 + (double)Fj[sjj + 3 * fs] * fj1) * sr;
+      const R* Msh = wk.Msh + x;
+      const double b1 = Msh[0], b2 = Msh[fs], b3 = Msh[2 * fs];
+      const double bsq = b1 * b1 + b2 * b2 + b3 * b3;
+      const double n22 = 0.5 * bsq - b2 * b2, n33 = 0.5 * bsq - b3 * b3;
+      sb[0] = 0.5 * (n22 + n33) * (fi1 - fi0) * ivol;
+      sb[1] = -((double)Fi[7 * fs] * fi0 + (double)Fi[si + 7 * fs] * fi1) * geo + (fj1 - fj0) * ivol * n33;
+      sb[2] = -((double)Fi[8 * fs] * fi0 + (double)Fi[si + 8 * fs] * fi1) * geo;
+      sb[2] += -((double)Fj[8 * fs] * fj0 + (double)Fj[sjj + 8 * fs] * fj1) * sr;
     }
-    // new face fields: this cell's lower faces and (for mags) the upper faces
+    // new face fields: this cell's lower faces and its upper faces
     double bl[3], bu[3];
+    bl[0] = ct_face<COORD, 0, R>(P, B, E, i, j, k, dt);
+    bl[1] = ct_face<COORD, 1, R>(P, B, E, i, j, k, dt);
+    bl[2] = ct_face<COORD, 2, R>(P, B, E, i, j, k, dt);
+    bu[0] = ct_face<COORD, 0, R>(P, B, E, i + 1, j, k, dt);
+    bu[1] = ct_face<COORD, 1, R>(P, B, E, i, j + 1, k, dt);
+    bu[2] = ct_face<COORD, 2, R>(P, B, E, i, j, k + 1, dt);
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-      bl[a] = ct_face<COORD, R>(P, B, E, a, i, j, k, dt);
-      bu[a] = ct_face<COORD, R>(P, B, E, a, i + (a == 0), j + (a == 1), k + (a == 2), dt);
       Bn[x + a * fs] = bl[a];
-      int pos = a == 0 ? i : (a == 1 ? j : k);
+      const int pos = a == 0 ? i : (a == 1 ? j : k);
       if (pos == NGH + P.n[a] - 1) Bn[x + stride(P, a) + a * fs] = bu[a];
     }
     // U^n from W^n (src/solver_func.c:356-382)
     const double gm1 = P.gm1;
-    double r0 = W[x], u0 = W[x + fs], v0 = W[x + 2 * fs], w0 = W[x + 3 * fs], p0 = W[x + 4 * fs],
-           ps0 = W[x + 5 * fs];
+    const double r0 = W[x], u0 = W[x + fs], v0 = W[x + 2 * fs], w0 = W[x + 3 * fs],
+                 p0 = W[x + 4 * fs], ps0 = W[x + 5 * fs];
     double U[6];
     U[0] = r0;
     U[1] = r0 * u0;
     U[2] = r0 * v0;
     U[3] = r0 * w0;
-    U[4] = 0.5 * r0 * (u0 * u0 + v0 * v0 + w0 * w0) + p0 / gm1;
-    U[5] = ps0 / pow(r0, gm1);
-    double U0[3] = {U[1], U[2], U[3]};
+    U[4] = 0.5 * r0 * (u0 * u0 + v0 * v0 + w0 * w0) + p0 * P.inv_gm1;
+    U[5] = (ps0 == 0.0 && r0 > 0.0) ? ps0 : ps0 / pow(r0, gm1);
+    const double U0[3] = {U[1], U[2], U[3]};
     // conservative update and cons->prim (src/solver_solve.c:326-377)
     U[0] -= dt * du[0];
 #pragma unroll
@@ -535,9 +540,10 @@ __global__ void k_update(Params P, Work<R> wk) {
     U[4] -= dt * du[4];
     U[5] -= dt * du[5];
     double rho = U[0];
-    double vv[3] = {U[1] / U[0], U[2] / U[0], U[3] / U[0]};
+    const double irho = 1.0 / U[0];
+    double vv[3] = {U[1] * irho, U[2] * irho, U[3] * irho};
     double p = (U[4] - 0.5 * (vv[0] * vv[0] + vv[1] * vv[1] + vv[2] * vv[2]) * rho) * gm1;
-    double pS = U[5] * pow(U[0], gm1);
+    const double pS = (U[5] == 0.0 && U[0] > 0.0) ? U[5] : U[5] * pow(U[0], gm1);
     // positivity floors (src/solver_func.c:2117-2135)
     if (rho < P.rho_floor) {
       rho = P.rho_floor;
@@ -546,20 +552,18 @@ __global__ void k_update(Params P, Work<R> wk) {
     if (p < P.p_floor) p = P.p_floor;
     // mags^{n+1}, time-centred field, Alfven/Boris correction
     // (src/solver_solve.c:385-484)
-    double mt[3];
+    double mt[3], mn[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-      int idx = a == 0 ? i : (a == 1 ? j : k);
-      double msn = bl[a] * tb(P, a, T_MA, idx) + bu[a] * tb(P, a, T_MB, idx);
-      double mso = mags_at(P, B, a, i, j, k);
-      mt[a] = 0.5 * (msn + mso);
-      bu[a] = msn;  // keep mags^{n+1} for the next dt
+      const int idx = a == 0 ? i : (a == 1 ? j : k);
+      mn[a] = bl[a] * tb(P, a, T_MA, idx) + bu[a] * tb(P, a, T_MB, idx);
+      mt[a] = 0.5 * (mn[a] + mags_at(P, B, a, i, j, k));
     }
-    double bsq = mt[0] * mt[0] + mt[1] * mt[1] + mt[2] * mt[2];
-    double alf = bsq / rho / P.ca2;
-    double perp = 1.0 / (1.0 + alf);
-    double drho = -dt * du[0];
-    double dva = alf * drho;
+    const double bsq = mt[0] * mt[0] + mt[1] * mt[1] + mt[2] * mt[2];
+    const double alf = bsq / rho / P.ca2;
+    const double perp = 1.0 / (1.0 + alf);
+    const double drho = -dt * du[0];
+    const double dva = alf * drho;
     double tv[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) tv[a] = alf * (-dt * du[1 + a] + dt * sh[a] - drho * W[x + (1 + a) * fs]);
@@ -567,9 +571,9 @@ __global__ void k_update(Params P, Work<R> wk) {
     bdv = bdv / (bsq + 1e-10);
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-      double mom = U0[a] + perp * ((-dt * du[1 + a] + dt * sh[a]) + (-dt * dm[a] + dt * sb[a]) +
-                                   dva * W[x + (1 + a) * fs] + mt[a] * bdv);
-      vv[a] = mom / U[0];
+      const double mom = U0[a] + perp * ((-dt * du[1 + a] + dt * sh[a]) + (-dt * dm[a] + dt * sb[a]) +
+                                         dva * W[x + (1 + a) * fs] + mt[a] * bdv);
+      vv[a] = mom * irho;
     }
     Wn[x] = rho;
     Wn[x + fs] = vv[0];
@@ -578,15 +582,9 @@ __global__ void k_update(Params P, Work<R> wk) {
     Wn[x + 4 * fs] = p;
     Wn[x + 5 * fs] = pS;
     // CFL dt of the new state (magtot = mags^{n+1}) and max|div B^{n+1}|
-    dtc = cfl_cell<COORD>(P, i, j, k, rho, vv[0], vv[1], vv[2], p, bu[0], bu[1], bu[2]);
-    double dvb = 0.0;
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-      int i1 = i + (a == 0), j1 = j + (a == 1), k1 = k + (a == 2);
-      // bu was overwritten with mags; recompute the upper face
-      double up = ct_face<COORD, R>(P, B, E, a, i1, j1, k1, dt);
-      dvb += (up * Geo<COORD>::face(P, a, i1, j1, k1) - bl[a] * Geo<COORD>::face(P, a, i, j, k)) / vol;
-    }
+    dtc = cfl_cell<COORD>(P, i, j, k, rho, vv[0], vv[1], vv[2], p, mn[0], mn[1], mn[2]);
+    const double dvb = (bu[0] * fu[0] - bl[0] * fl[0]) * ivol + (bu[1] * fu[1] - bl[1] * fl[1]) * ivol +
+                       (bu[2] * fu[2] - bl[2] * fl[2]) * ivol;
     dbmax = fabs(dvb);
     if (!(dtc > 0.0) || !isfinite(p) || !isfinite(rho) || !isfinite(vv[0] + vv[1] + vv[2]))
       P.scal[S_FLAGS] = 1.0;
@@ -745,6 +743,30 @@ void launch_dt(const Params& P, int coord, cudaStream_t st) {
   else LAUNCH(k_dt<2>, g, blk, st, P);
 }
 
+template <typename R, int D>
+static void launch_dir(const Params& P, const Work<R>& w, cudaStream_t st, int which) {
+  constexpr int p = (D + 1) % 3, q = (D + 2) % 3;
+  dim3 blk(32, 4, 2);
+  int cnt[3];
+  if (which == 0) {  // first centre-to-edge sweep
+    cnt[D] = P.n[D];
+    cnt[p] = P.n[p] + 1;
+    cnt[q] = P.n[q] + 2 * NGH;
+    LAUNCH((k_c2c<R, D>), grid3(cnt[0], cnt[1], cnt[2], blk), blk, st, P, w);
+  } else if (which == 1) {  // edge EMF
+    cnt[D] = P.n[D];
+    cnt[p] = P.n[p] + 1;
+    cnt[q] = P.n[q] + 1;
+    LAUNCH((k_emf<R, D>), grid3(cnt[0], cnt[1], cnt[2], blk), blk, st, P, w);
+  } else {  // face flux
+    cnt[0] = P.n[0];
+    cnt[1] = P.n[1];
+    cnt[2] = P.n[2];
+    cnt[D] += 1;
+    LAUNCH((k_flux<R, D>), grid3(cnt[0], cnt[1], cnt[2], blk), blk, st, P, w);
+  }
+}
+
 template <typename R>
 void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t st,
                       const Hook& hook) {
@@ -752,33 +774,14 @@ void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t
   hook(G_AB2, 1);
   LAUNCH(k_ab2<R>, grid3(P.N[0], P.N[1], P.N[2], blk), blk, st, P, w);
   hook(G_AB2, 0);
-  hook(G_C2C, 1);
-  for (int d = 0; d < 3; d++) {
-    int p = (d + 1) % 3, q = (d + 2) % 3;
-    int cnt[3];
-    cnt[d] = P.n[d];
-    cnt[p] = P.n[p] + 1;
-    cnt[q] = P.n[q] + 2 * NGH;
-    LAUNCH(k_c2c<R>, grid3(cnt[0], cnt[1], cnt[2], blk), blk, st, P, d, w);
+  for (int stage = 0; stage < 3; stage++) {
+    int g = stage == 0 ? G_C2C : (stage == 1 ? G_EMF : G_FLUX);
+    hook(g, 1);
+    launch_dir<R, 0>(P, w, st, stage);
+    launch_dir<R, 1>(P, w, st, stage);
+    launch_dir<R, 2>(P, w, st, stage);
+    hook(g, 0);
   }
-  hook(G_C2C, 0);
-  hook(G_EMF, 1);
-  for (int d = 0; d < 3; d++) {
-    int p = (d + 1) % 3, q = (d + 2) % 3;
-    int cnt[3];
-    cnt[d] = P.n[d];
-    cnt[p] = P.n[p] + 1;
-    cnt[q] = P.n[q] + 1;
-    LAUNCH(k_emf<R>, grid3(cnt[0], cnt[1], cnt[2], blk), blk, st, P, d, w);
-  }
-  hook(G_EMF, 0);
-  hook(G_FLUX, 1);
-  for (int d = 0; d < 3; d++) {
-    int cnt[3] = {P.n[0], P.n[1], P.n[2]};
-    cnt[d] += 1;
-    LAUNCH(k_flux<R>, grid3(cnt[0], cnt[1], cnt[2], blk), blk, st, P, d, w);
-  }
-  hook(G_FLUX, 0);
   hook(G_UPDATE, 1);
   dim3 ub(32, 4, 2);
   if (coord == 0)
