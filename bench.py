@@ -38,6 +38,9 @@ METRIC = "Mcell-updates/s vs plain FP64 GPU at fixed L1 err; %HBM peak; p50/p99 
 UNIT = "Mcell-updates/s"
 BYTES_PER_CELL_UPDATE = 216  # algorithmic bytes of one cell-update (FP64)
 GROUP_LAUNCHES = {"ab2": 1, "c2c": 3, "emf": 3, "flux": 3, "update": 1}
+# thread-block shapes the library's autotuner chooses from (gop_autotune)
+BLOCK_CANDIDATES = ["32x4x2", "32x8x1", "32x1x8", "32x2x4", "64x2x2", "64x4x1", "64x1x4",
+                    "128x2x1", "128x1x2", "32x4x1", "64x2x1", "256x1x1"]
 
 
 def peaks():
@@ -189,6 +192,7 @@ def main():
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -227,6 +231,7 @@ def main():
     inst = gop.make(gop.PROBLEM_BLAST, n, precision=prec)
     inst.set_stream(stream.cuda_stream)
     inst.prepare()
+    tuned = None if args.no_autotune else inst.autotune(reps=2)
     with torch.cuda.stream(stream):
         inst.step(args.warmup)
         torch.cuda.synchronize()
@@ -281,7 +286,8 @@ def main():
                    "problem": "blast p_in=10 p_out=0.1 r=0.1 B=(1/sqrt2,1/sqrt2,0) gamma=5/3 CFL=0.3",
                    "parallelism": f"replicas x{world} (no data-path collective)",
                    "l2": "state 2.4 GB per replica >> 126 MB L2, no flush needed",
-                   "precision": args.precision},
+                   "precision": args.precision,
+                   "block_shapes": ({k: BLOCK_CANDIDATES[v] for k, v in tuned.items()} if tuned else "defaults")},
         "latency_ms": {"p50": round(float(np.percentile(durs, 50)), 4),
                        "p99": round(float(np.percentile(durs, 99)), 4)},
         "roofline": {"bound": "hbm", "kernel": f"k_{dom}", "achieved": round(achieved, 2),

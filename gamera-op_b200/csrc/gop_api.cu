@@ -329,6 +329,7 @@ struct gop_instance {
   double* hscal = nullptr;   // pinned host copy of the scalars
   Work<double> wd;
   Work<float> wf;
+  Tune tune;
   size_t bytes = 0;
   bool prepared = false;
   // per-kernel-group event timing (gop_set_profiling)
@@ -597,9 +598,9 @@ static int enqueue_steps(gop_instance* h, int nsteps, double time_stop) {
     launch_begin(P, h->st);
     hook(G_BEGIN, 0);
     if (h->d.precision == GOP_PREC_MIXED)
-      launch_step_body<float>(P, h->d.coord, h->wf, h->st, hook);
+      launch_step_body<float>(P, h->d.coord, h->wf, h->st, h->tune, hook);
     else
-      launch_step_body<double>(P, h->d.coord, h->wd, h->st, hook);
+      launch_step_body<double>(P, h->d.coord, h->wd, h->st, h->tune, hook);
     hook(G_GHOST, 1);
     launch_ghosts(P, h->d.bc, h->d.gem_bc, 0, h->st);
     hook(G_GHOST, 0);
@@ -687,6 +688,70 @@ int gop_download(gop_instance* h, double* gas, double* face_b, double* gas_h, do
   if (mags_p) rc = mixed ? download_work<float>(h, 3, h->wf.Ms, mags_p) : download_field(h, 3, h->wd.Ms, mags_p);
   CK(cudaGetLastError());
   return rc;
+}
+
+// Project-written autotuner: for each tunable kernel, time a set of block
+// shapes on the instance's current state (these kernels are pure functions of
+// the current buffers, so re-running them does not change the state) and
+// keep the fastest.  The prepared state must be valid (after gop_prepare).
+int gop_autotune(gop_instance* h, int reps, int* chosen) {
+  if (!h) return fail(GOP_EINVAL, "instance is NULL");
+  if (!h->prepared) return fail(GOP_ESTATE, "gop_prepare must run before gop_autotune");
+  if (reps <= 0) reps = 3;
+  static const dim3 cand[] = {dim3(32, 4, 2), dim3(32, 8, 1), dim3(32, 1, 8), dim3(32, 2, 4),
+                              dim3(64, 2, 2), dim3(64, 4, 1), dim3(64, 1, 4), dim3(128, 2, 1),
+                              dim3(128, 1, 2), dim3(32, 4, 1), dim3(64, 2, 1), dim3(256, 1, 1)};
+  const int ncand = sizeof(cand) / sizeof(cand[0]);
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  // k_update writes the next state into the history buffers: keep a copy of
+  // them and of the device scalars, and put both back afterwards
+  const Params& P = h->P;
+  int cur = 0;
+  CK(cudaMemcpyAsync(h->hscal, h->scal, NSCAL * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  std::vector<double> saved_scal(h->hscal, h->hscal + NSCAL);
+  cur = saved_scal[S_PAR] != 0.0 ? 1 : 0;
+  double* hist = nullptr;
+  const size_t wbytes = (size_t)P.fs * 6 * sizeof(double), bbytes = (size_t)P.fs * 3 * sizeof(double);
+  CK(cudaMalloc((void**)&hist, wbytes + bbytes));
+  CK(cudaMemcpyAsync(hist, P.Wbuf[1 - cur], wbytes, cudaMemcpyDeviceToDevice, h->st));
+  CK(cudaMemcpyAsync(hist + 6 * P.fs, P.Bbuf[1 - cur], bbytes, cudaMemcpyDeviceToDevice, h->st));
+  const bool mixed = h->d.precision == GOP_PREC_MIXED;
+  for (int slot = 0; slot < NTUNE; slot++) {
+    float best = 1e30f;
+    int best_c = 0;
+    for (int c = 0; c < ncand; c++) {
+      if (cand[c].x * cand[c].y * cand[c].z > 256) continue;
+      // warm-up launch, then reps timed launches
+      for (int r = 0; r <= reps; r++) {
+        if (r == 1) cudaEventRecord(a, h->st);
+        if (mixed) launch_slot<float>(h->P, h->d.coord, h->wf, slot, cand[c], h->st);
+        else launch_slot<double>(h->P, h->d.coord, h->wd, slot, cand[c], h->st);
+      }
+      cudaEventRecord(b, h->st);
+      CK(cudaEventSynchronize(b));
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, a, b);
+      if (ms < best) {
+        best = ms;
+        best_c = c;
+      }
+    }
+    h->tune.blk[slot] = cand[best_c];
+    if (chosen) chosen[slot] = best_c;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  CK(cudaMemcpyAsync(P.Wbuf[1 - cur], hist, wbytes, cudaMemcpyDeviceToDevice, h->st));
+  CK(cudaMemcpyAsync(P.Bbuf[1 - cur], hist + 6 * P.fs, bbytes, cudaMemcpyDeviceToDevice, h->st));
+  for (int t = 0; t < NSCAL; t++) h->hscal[t] = saved_scal[t];
+  CK(cudaMemcpyAsync(h->scal, h->hscal, NSCAL * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  cudaFree(hist);
+  CK(cudaGetLastError());
+  return GOP_OK;
 }
 
 int gop_set_profiling(gop_instance* h, int on) {

@@ -743,10 +743,18 @@ void launch_dt(const Params& P, int coord, cudaStream_t st) {
   else LAUNCH(k_dt<2>, g, blk, st, P);
 }
 
+Tune::Tune() {
+  // defaults: warps along i; the sweep of D=1 / D=2 kernels runs along the
+  // block's longer transverse side so neighbouring rows share L1 lines
+  for (int t = 0; t < NTUNE; t++) blk[t] = dim3(32, 4, 2);
+  blk[K_C2C0] = blk[K_EMF0] = blk[K_FLUX0] = dim3(32, 4, 2);
+  blk[K_C2C1] = blk[K_EMF1] = blk[K_FLUX1] = dim3(32, 8, 1);
+  blk[K_C2C2] = blk[K_EMF2] = blk[K_FLUX2] = dim3(32, 1, 8);
+}
+
 template <typename R, int D>
-static void launch_dir(const Params& P, const Work<R>& w, cudaStream_t st, int which) {
+static void launch_dir(const Params& P, const Work<R>& w, cudaStream_t st, int which, dim3 blk) {
   constexpr int p = (D + 1) % 3, q = (D + 2) % 3;
-  dim3 blk(32, 4, 2);
   int cnt[3];
   if (which == 0) {  // first centre-to-edge sweep
     cnt[D] = P.n[D];
@@ -768,33 +776,50 @@ static void launch_dir(const Params& P, const Work<R>& w, cudaStream_t st, int w
 }
 
 template <typename R>
+void launch_slot(const Params& P, int coord, const Work<R>& w, int slot, dim3 blk,
+                 cudaStream_t st) {
+  if (slot == K_AB2) {
+    LAUNCH(k_ab2<R>, grid3(P.N[0], P.N[1], P.N[2], blk), blk, st, P, w);
+  } else if (slot == K_UPDATE) {
+    if (coord == 0)
+      LAUNCH((k_update<0, R>), grid3(P.n[0], P.n[1], P.n[2], blk), blk, st, P, w);
+    else
+      LAUNCH((k_update<2, R>), grid3(P.n[0], P.n[1], P.n[2], blk), blk, st, P, w);
+  } else {
+    int stage = (slot - K_C2C0) / 3, d = (slot - K_C2C0) % 3;
+    if (d == 0) launch_dir<R, 0>(P, w, st, stage, blk);
+    else if (d == 1) launch_dir<R, 1>(P, w, st, stage, blk);
+    else launch_dir<R, 2>(P, w, st, stage, blk);
+  }
+}
+
+template void launch_slot<double>(const Params&, int, const Work<double>&, int, dim3, cudaStream_t);
+template void launch_slot<float>(const Params&, int, const Work<float>&, int, dim3, cudaStream_t);
+
+template <typename R>
 void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t st,
-                      const Hook& hook) {
-  dim3 blk(32, 4, 2);
+                      const Tune& tune, const Hook& hook) {
   hook(G_AB2, 1);
-  LAUNCH(k_ab2<R>, grid3(P.N[0], P.N[1], P.N[2], blk), blk, st, P, w);
+  launch_slot<R>(P, coord, w, K_AB2, tune.blk[K_AB2], st);
   hook(G_AB2, 0);
   for (int stage = 0; stage < 3; stage++) {
     int g = stage == 0 ? G_C2C : (stage == 1 ? G_EMF : G_FLUX);
     hook(g, 1);
-    launch_dir<R, 0>(P, w, st, stage);
-    launch_dir<R, 1>(P, w, st, stage);
-    launch_dir<R, 2>(P, w, st, stage);
+    for (int d = 0; d < 3; d++) {
+      int slot = K_C2C0 + 3 * stage + d;
+      launch_slot<R>(P, coord, w, slot, tune.blk[slot], st);
+    }
     hook(g, 0);
   }
   hook(G_UPDATE, 1);
-  dim3 ub(32, 4, 2);
-  if (coord == 0)
-    LAUNCH((k_update<0, R>), grid3(P.n[0], P.n[1], P.n[2], ub), ub, st, P, w);
-  else
-    LAUNCH((k_update<2, R>), grid3(P.n[0], P.n[1], P.n[2], ub), ub, st, P, w);
+  launch_slot<R>(P, coord, w, K_UPDATE, tune.blk[K_UPDATE], st);
   hook(G_UPDATE, 0);
 }
 
 template void launch_step_body<double>(const Params&, int, const Work<double>&, cudaStream_t,
-                                       const Hook&);
+                                       const Tune&, const Hook&);
 template void launch_step_body<float>(const Params&, int, const Work<float>&, cudaStream_t,
-                                      const Hook&);
+                                      const Tune&, const Hook&);
 
 void launch_ghosts(const Params& P, const char bc[6], const char gem_bc[6], int which,
                    cudaStream_t st) {

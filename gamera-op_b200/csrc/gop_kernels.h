@@ -26,6 +26,19 @@ int64_t launches();
 // kernel groups of one step, for event timing
 enum Group : int { G_BEGIN = 0, G_AB2, G_C2C, G_EMF, G_FLUX, G_UPDATE, G_GHOST, G_END, NGROUP };
 
+// launch shapes of the tunable kernels: AB2, C2C x3, EMF x3, FLUX x3, UPDATE
+enum TuneSlot : int { K_AB2 = 0, K_C2C0, K_C2C1, K_C2C2, K_EMF0, K_EMF1, K_EMF2,
+                      K_FLUX0, K_FLUX1, K_FLUX2, K_UPDATE, NTUNE };
+struct Tune {
+  dim3 blk[NTUNE];
+  Tune();
+};
+
+// launches one tunable kernel alone (for the autotuner)
+template <typename R>
+void launch_slot(const Params& P, int coord, const Work<R>& w, int slot, dim3 blk,
+                 cudaStream_t st);
+
 // optional timing hook: mark(ctx, group, start) records an event on the stream
 struct Hook {
   void (*mark)(void* ctx, int group, int start) = nullptr;
@@ -40,7 +53,7 @@ void launch_arm(const Params& P, double tstop, cudaStream_t st);
 void launch_dt(const Params& P, int coord, cudaStream_t st);
 template <typename R>
 void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t st,
-                      const Hook& hook = Hook());
+                      const Tune& tune, const Hook& hook = Hook());
 // which = 0: the buffer being written this step; 1: the current state
 void launch_ghosts(const Params& P, const char bc[6], const char gem_bc[6], int which,
                    cudaStream_t st);

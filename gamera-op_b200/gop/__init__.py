@@ -90,6 +90,7 @@ def lib():
         L.gop_grid_uniform.argtypes = [C.c_int, C.c_double, C.c_double, _dp]
         L.gop_problem_defaults.argtypes = [C.c_int, C.POINTER(Problem)]
         L.gop_problem_init.argtypes = [C.POINTER(Desc), C.POINTER(Problem), _dp, _dp]
+        L.gop_autotune.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
         L.gop_set_profiling.argtypes = [vp, C.c_int]
         L.gop_get_profile.argtypes = [vp, _dp, C.POINTER(C.c_int64)]
         L.gop_batch_create.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(vp)]
@@ -227,6 +228,15 @@ class Instance:
         return out
 
     GROUPS = ("begin", "ab2", "c2c", "emf", "flux", "update", "ghost", "end")
+    TUNE_SLOTS = ("ab2", "c2c_i", "c2c_j", "c2c_k", "emf_i", "emf_j", "emf_k", "flux_i",
+                  "flux_j", "flux_k", "update")
+
+    def autotune(self, reps=3) -> dict:
+        """Times candidate block shapes per launch on the current state and
+        keeps the fastest; returns the chosen candidate index per launch."""
+        out = (C.c_int * len(self.TUNE_SLOTS))()
+        _check(lib().gop_autotune(self._h, int(reps), out))
+        return dict(zip(self.TUNE_SLOTS, list(out)))
 
     def set_profiling(self, on: bool):
         _check(lib().gop_set_profiling(self._h, int(bool(on))))

@@ -128,6 +128,14 @@ int gop_download(gop_instance *h, double *gas, double *face_b, double *gas_h,
 
 int gop_get_stats(gop_instance *h, gop_stats *out);
 
+/* Autotuner: times candidate thread-block shapes for each of the 11
+ * tunable launches of a step on the instance's current state (after
+ * gop_prepare; the state is not advanced) and keeps the fastest for the
+ * following steps.  reps: timed launches per candidate (0 = 3); chosen
+ * (optional, 11 ints) receives the picked candidate index per launch. */
+#define GOP_NTUNE 11
+int gop_autotune(gop_instance *h, int reps, int *chosen);
+
 /* Diagnostics: time every kernel group of every step with CUDA events on
  * the instance's stream (off by default; switching resets the totals).
  * Groups: 0 begin, 1 ab2, 2 centre-to-edge, 3 edge EMF, 4 face flux,
