@@ -431,6 +431,7 @@ int gop_create(const gop_desc* desc, gop_instance** out) {
   P.n[2] = d.nk;
   for (int a = 0; a < 3; a++) P.N[a] = L.N[a];
   P.pitch = L.pitch;
+  P.coord = d.coord;
   P.sj = L.pitch;
   P.sk = (long long)L.pitch * L.N[1];
   P.fs = L.fs;
@@ -592,7 +593,7 @@ static int enqueue_steps(gop_instance* h, int nsteps, double time_stop) {
     hook.mark = prof_mark;
     hook.ctx = h;
   }
-  launch_arm(P, time_stop, h->st);
+  launch_arm(P, time_stop, (double)nsteps, h->st);
   for (int n = 0; n < nsteps; n++) {
     hook(G_BEGIN, 1);
     launch_begin(P, h->st);
@@ -798,36 +799,151 @@ int gop_get_stats(gop_instance* h, gop_stats* out) {
 
 }  // extern "C"
 
-#include <map>
+// A batch advances many independent grids with one launch per stage: the
+// blocks of every member's launch of a stage are concatenated into one work
+// list, so small grids that could not fill the GPU alone fill it together.
+// Each member keeps its own device scalars (dt, time, AB2 coefficient, step
+// budget); one captured batched step is replayed max(steps) times and a
+// member whose budget is spent skips the rest.
+struct BatchSide {
+  int n = 0;
+  void* members = nullptr;  // device Member<R>[n]
+  BatchLists L{};
+  int* steps = nullptr;     // device int[n]
+};
 
 struct gop_batch {
   std::vector<gop_instance*> m;
+  std::vector<int> idx[2];  // member indices per precision (0: FP64, 1: mixed)
+  BatchSide side[2];
+  void* dev = nullptr;      // one device allocation for members, lists and steps
+  int* hsteps = nullptr;    // pinned staging of the step budgets
   cudaStream_t st = nullptr;
-  std::vector<cudaStream_t> lanes;
-  std::vector<cudaEvent_t> ev;
-  cudaEvent_t fork = nullptr;
-  std::map<std::vector<int>, cudaGraphExec_t> graphs;
+  cudaGraphExec_t graph = nullptr;
 };
+
+static int batch_slot_used(const gop_instance* h, int slot) {
+  const char* bc = h->d.bc;
+  const char* gbc = h->d.gem_bc;
+  if (slot < NTUNE) return 1;
+  if (slot <= K_WRAP2) {
+    const int a = slot - K_WRAP0;
+    return bc[2 * a] == 'p' && bc[2 * a + 1] == 'p';
+  }
+  const int face = slot - K_BC0, a = face / 2;
+  if (bc[2 * a] == 'p' && bc[2 * a + 1] == 'p') return 0;
+  const bool gas_work = bc[face] != 'n';
+  const bool gem_work = gbc[face] != 'n' && gbc[face] != 'r';
+  return gas_work || gem_work;
+}
+
+static dim3 batch_block(int slot) {
+  static const Tune defaults;
+  return slot < NTUNE ? defaults.blk[slot] : dim3(32, 8, 1);
+}
 
 extern "C" {
 
 int gop_batch_create(gop_instance* const* members, int count, gop_batch** out) {
   if (!members || count <= 0 || !out) return fail(GOP_EINVAL, "bad batch arguments");
+  if (count > 0xffff) return fail(GOP_EINVAL, "at most 65535 members per batch");
   *out = nullptr;
   for (int i = 0; i < count; i++) {
     if (!members[i]) return fail(GOP_EINVAL, "member %d is NULL", i);
     if (!members[i]->prepared) return fail(GOP_ESTATE, "member %d is not prepared", i);
+    for (int k = 0; k < i; k++)
+      if (members[k] == members[i]) return fail(GOP_EINVAL, "member %d appears twice", i);
   }
   gop_batch* b = new (std::nothrow) gop_batch();
   if (!b) return fail(GOP_ENOMEM, "host allocation failed");
   b->m.assign(members, members + count);
-  CK(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
-  CK(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
-  b->lanes.resize(count);
-  b->ev.resize(count);
-  for (int i = 0; i < count; i++) {
-    CK(cudaStreamCreateWithFlags(&b->lanes[i], cudaStreamNonBlocking));
-    CK(cudaEventCreateWithFlags(&b->ev[i], cudaEventDisableTiming));
+  for (int i = 0; i < count; i++) b->idx[members[i]->d.precision == GOP_PREC_MIXED ? 1 : 0].push_back(i);
+
+  // host images: members, then per slot the work items, then step budgets
+  std::vector<unsigned long long> items[2][NSLOT];
+  std::vector<Member<double>> md;
+  std::vector<Member<float>> mf;
+  for (int s = 0; s < 2; s++) {
+    for (int li = 0; li < (int)b->idx[s].size(); li++) {
+      gop_instance* h = members[b->idx[s][li]];
+      if (s == 0) {
+        Member<double> M{};
+        M.P = h->P;
+        M.w = h->wd;
+        for (int f = 0; f < 6; f++) M.bc[f] = h->d.bc[f], M.gbc[f] = h->d.gem_bc[f];
+        md.push_back(M);
+      } else {
+        Member<float> M{};
+        M.P = h->P;
+        M.w = h->wf;
+        for (int f = 0; f < 6; f++) M.bc[f] = h->d.bc[f], M.gbc[f] = h->d.gem_bc[f];
+        mf.push_back(M);
+      }
+      for (int slot = 0; slot < NSLOT; slot++) {
+        if (!batch_slot_used(h, slot)) continue;
+        const dim3 sp = launch_space(h->P, slot), blk = batch_block(slot);
+        const unsigned gx = (sp.x + blk.x - 1) / blk.x, gy = (sp.y + blk.y - 1) / blk.y,
+                       gz = (sp.z + blk.z - 1) / blk.z;
+        if (gx > 0xffff || gy > 0xffff || gz > 0xffff) {
+          delete b;
+          return fail(GOP_EINVAL, "member %d is too large for a batch", b->idx[s][li]);
+        }
+        for (unsigned z = 0; z < gz; z++)
+          for (unsigned y = 0; y < gy; y++)
+            for (unsigned x = 0; x < gx; x++)
+              items[s][slot].push_back(((unsigned long long)li << 48) | ((unsigned long long)x << 32) |
+                                       ((unsigned long long)y << 16) | z);
+      }
+    }
+  }
+  size_t off = 0;
+  auto place = [&](size_t bytes) {
+    size_t o = (off + 255) & ~(size_t)255;
+    off = o + bytes;
+    return o;
+  };
+  size_t o_mem[2], o_items[2][NSLOT], o_steps[2];
+  o_mem[0] = place(md.size() * sizeof(Member<double>));
+  o_mem[1] = place(mf.size() * sizeof(Member<float>));
+  for (int s = 0; s < 2; s++) {
+    for (int slot = 0; slot < NSLOT; slot++) o_items[s][slot] = place(items[s][slot].size() * 8);
+    o_steps[s] = place(b->idx[s].size() * sizeof(int));
+  }
+  cudaError_t e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&b->dev, off);
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&b->hsteps, count * sizeof(int));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    gop_batch_destroy(b);
+    return fail(GOP_ENOMEM, "batch allocation of %zu bytes failed: %s", off, cudaGetErrorString(e));
+  }
+  char* base = (char*)b->dev;
+  CK(cudaMemcpy(base + o_mem[0], md.data(), md.size() * sizeof(Member<double>), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(base + o_mem[1], mf.data(), mf.size() * sizeof(Member<float>), cudaMemcpyHostToDevice));
+  for (int s = 0; s < 2; s++) {
+    BatchSide& S = b->side[s];
+    S.n = (int)b->idx[s].size();
+    S.members = base + o_mem[s];
+    S.steps = (int*)(base + o_steps[s]);
+    for (int slot = 0; slot < NSLOT; slot++) {
+      CK(cudaMemcpy(base + o_items[s][slot], items[s][slot].data(), items[s][slot].size() * 8,
+                    cudaMemcpyHostToDevice));
+      S.L.count[slot] = (int)items[s][slot].size();
+      S.L.blk[slot] = batch_block(slot);
+      S.L.items[slot] = (const unsigned long long*)(base + o_items[s][slot]);
+    }
+  }
+  // one batched step of every member, captured once
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+  if (b->side[0].n) launch_batch_step<double>((const Member<double>*)b->side[0].members, b->side[0].n, b->side[0].L, b->st);
+  if (b->side[1].n) launch_batch_step<float>((const Member<float>*)b->side[1].members, b->side[1].n, b->side[1].L, b->st);
+  e = cudaStreamEndCapture(b->st, &g);
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&b->graph, g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    gop_batch_destroy(b);
+    return fail(GOP_ECUDA, "batch graph capture failed: %s", cudaGetErrorString(e));
   }
   *out = b;
   return GOP_OK;
@@ -836,55 +952,40 @@ int gop_batch_create(gop_instance* const* members, int count, gop_batch** out) {
 int gop_batch_destroy(gop_batch* b) {
   if (!b) return GOP_OK;
   if (b->st) cudaStreamSynchronize(b->st);
-  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
-  for (size_t i = 0; i < b->lanes.size(); i++) {
-    cudaStreamDestroy(b->lanes[i]);
-    cudaEventDestroy(b->ev[i]);
-  }
-  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->dev) cudaFree(b->dev);
+  if (b->hsteps) cudaFreeHost(b->hsteps);
   if (b->st) cudaStreamDestroy(b->st);
   delete b;
   return GOP_OK;
 }
 
-// One graph per distinct step vector: each member's steps form an
-// independent branch (fork / join through events), so the small grids of a
-// batch run concurrently from a single graph launch.
 int gop_batch_step(gop_batch* b, const int* steps) {
   if (!b || !steps) return fail(GOP_EINVAL, "NULL argument");
-  std::vector<int> key(steps, steps + b->m.size());
-  for (int v : key)
-    if (v < 0) return fail(GOP_EINVAL, "negative step count");
-  auto it = b->graphs.find(key);
-  if (it == b->graphs.end()) {
-    cudaGraph_t g = nullptr;
-    CK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
-    cudaEventRecord(b->fork, b->st);
-    std::vector<cudaStream_t> saved(b->m.size());
-    int rc = GOP_OK;
-    for (size_t i = 0; i < b->m.size() && rc == GOP_OK; i++) {
-      cudaStreamWaitEvent(b->lanes[i], b->fork, 0);
-      saved[i] = b->m[i]->st;
-      b->m[i]->st = b->lanes[i];
-      rc = enqueue_steps(b->m[i], key[i], 1e300);
-      b->m[i]->st = saved[i];
-      cudaEventRecord(b->ev[i], b->lanes[i]);
-      cudaStreamWaitEvent(b->st, b->ev[i], 0);
-    }
-    cudaError_t e = cudaStreamEndCapture(b->st, &g);
-    if (rc) {
-      if (g) cudaGraphDestroy(g);
-      return rc;
-    }
-    if (e != cudaSuccess) return fail(GOP_ECUDA, "graph capture failed: %s", cudaGetErrorString(e));
-    cudaGraphExec_t x = nullptr;
-    e = cudaGraphInstantiate(&x, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) return fail(GOP_ECUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
-    it = b->graphs.emplace(key, x).first;
+  int most = 0;
+  for (size_t i = 0; i < b->m.size(); i++) {
+    if (steps[i] < 0) return fail(GOP_EINVAL, "negative step count");
+    most = std::max(most, steps[i]);
   }
-  CK(cudaGraphLaunch(it->second, b->st));
+  // members' own streams may still hold work on their state
+  for (gop_instance* h : b->m) CK(cudaStreamSynchronize(h->st));
+  for (int s = 0; s < 2; s++) {
+    BatchSide& S = b->side[s];
+    if (!S.n) continue;
+    int* hs = b->hsteps + (s == 0 ? 0 : b->side[0].n);
+    for (int li = 0; li < S.n; li++) hs[li] = steps[b->idx[s][li]];
+    CK(cudaMemcpyAsync(S.steps, hs, S.n * sizeof(int), cudaMemcpyHostToDevice, b->st));
+    if (s == 0) launch_batch_arm<double>((const Member<double>*)S.members, S.n, S.steps, b->st);
+    else launch_batch_arm<float>((const Member<float>*)S.members, S.n, S.steps, b->st);
+  }
+  for (int n = 0; n < most; n++) CK(cudaGraphLaunch(b->graph, b->st));
   CK(cudaStreamSynchronize(b->st));
+  CK(cudaGetLastError());
+  for (gop_instance* h : b->m) {
+    double* sc = h->hscal;
+    CK(cudaMemcpy(sc, h->scal, NSCAL * sizeof(double), cudaMemcpyDeviceToHost));
+    if (sc[S_FLAGS] != 0.0) return fail(GOP_ENUMERIC, "non-finite or non-positive state in a member");
+  }
   return GOP_OK;
 }
 

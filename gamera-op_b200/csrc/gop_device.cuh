@@ -55,6 +55,7 @@ enum Scal : int {
   S_TSTOP,       // time_stop of the current gop_step call
   S_FLAGS,       // bit 0: non-finite / non-positive state seen
   S_PAR,         // which of the two state buffers holds the current state
+  S_BUDGET,      // steps left in the current gop_step call
   NSCAL
 };
 
@@ -62,6 +63,7 @@ struct Params {
   int n[3];           // active cells
   int N[3];           // ghost-extended points
   int pitch;          // row pitch (elements)
+  int coord;          // 0: Cartesian, 2: spherical (batched kernels select on it)
   long long sj, sk;   // strides of j and k (stride of i is 1)
   long long fs;       // stride between fields
   const double* tab;  // [3][NTAB][tmax]

@@ -13,6 +13,12 @@
 //   update    divergence, sources, constrained transport, cons->prim,
 //             floors, Alfven/Boris correction, next CFL dt, max|div B|
 //   ghost     periodic wrap and boundary fills of the new state
+//   end       the written buffer becomes the current state
+//
+// Every stage is a per-point body function used by two kernel forms: a
+// single-instance kernel (the launch grid covers one grid) and a batched
+// kernel whose blocks come from a work list of (instance, block) items, so
+// one launch advances every member of a batch of uneven grids.
 //
 // R is the arithmetic type of the reconstruction / flux / EMF stages
 // (double: plain path; float: mixed path).  The state, the AB2
@@ -50,14 +56,12 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
-// block-wide min and max of (a, b); thread 0 commits them with one atomic each
+// block-wide min and max of (a, b); one thread commits them with one atomic each
 __device__ __forceinline__ void block_commit(double a, double b, double* smin, double* smax) {
   __shared__ double sa[32], sb[32];
-  int lane = threadIdx.x & 31;
-  int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
-  int nw = (blockDim.x * blockDim.y * blockDim.z + 31) / 32;
-  int w = tid / 32;
-  lane = tid & 31;
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nw = (blockDim.x * blockDim.y * blockDim.z + 31) / 32;
+  const int w = tid / 32, lane = tid & 31;
   a = warp_min(a);
   b = warp_max(b);
   if (lane == 0) {
@@ -102,117 +106,6 @@ __device__ __forceinline__ double mags_at(const Params& P, const double* B, int 
   return f[c] * tb(P, a, T_MA, idx) + f[c + stride(P, a)] * tb(P, a, T_MB, idx);
 }
 
-// ------------------------------------------------------------ begin / dt
-
-// one thread: open the step (src/solver_solve.c:103-107, solver_func.c:385-491)
-__global__ void k_begin(Params P) {
-  double* s = P.scal;
-  if (s[S_STOP] != 0.0) return;
-  if (s[S_TIME] > s[S_TSTOP]) {
-    s[S_STOP] = 1.0;
-    return;
-  }
-  double dt = __longlong_as_double((long long)__double_as_longlong(s[S_NEXT_DT]));
-  if (!(dt > 0.0) || !isfinite(dt)) s[S_FLAGS] = 1.0;
-  s[S_DT] = dt;
-  s[S_TIME] = s[S_TIME] + dt;
-  s[S_CAB2] = 0.5 * dt / s[S_DT0];
-  s[S_DT0] = dt;
-  s[S_NEXT_DT] = DBL_MAX;
-  s[S_DIVB] = 0.0;
-  s[S_STEPS] = s[S_STEPS] + 1.0;
-}
-
-// one thread: arm a gop_step call with its stop time
-__global__ void k_arm(Params P, double tstop) {
-  P.scal[S_TSTOP] = tstop;
-  P.scal[S_STOP] = 0.0;
-}
-
-// one thread: close the step -- the buffer written by this step becomes
-// the current state
-__global__ void k_end(Params P) {
-  if (P.scal[S_STOP] != 0.0) return;
-  P.scal[S_PAR] = P.scal[S_PAR] != 0.0 ? 0.0 : 1.0;
-}
-
-// CFL dt and max|div B| of the current state (used by prepare)
-template <int COORD>
-__global__ void k_dt(Params P) {
-  const double* __restrict__ W = P.Wbuf[cur_buf(P)];
-  const double* __restrict__ B = P.Bbuf[cur_buf(P)];
-  int i = NGH + blockIdx.x * blockDim.x + threadIdx.x;
-  int j = NGH + blockIdx.y * blockDim.y + threadIdx.y;
-  int k = NGH + blockIdx.z * blockDim.z + threadIdx.z;
-  double dtc = DBL_MAX, db = 0.0;
-  if (i < NGH + P.n[0] && j < NGH + P.n[1] && k < NGH + P.n[2]) {
-    long long c = lin(P, i, j, k);
-    double b1 = mags_at(P, B, 0, i, j, k), b2 = mags_at(P, B, 1, i, j, k),
-           b3 = mags_at(P, B, 2, i, j, k);
-    dtc = cfl_cell<COORD>(P, i, j, k, W[c], W[c + P.fs], W[c + 2 * P.fs], W[c + 3 * P.fs],
-                          W[c + 4 * P.fs], b1, b2, b3);
-    double vol = Geo<COORD>::vol(P, i, j, k), d = 0.0;
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-      const double* f = B + (size_t)a * P.fs;
-      long long s = stride(P, a);
-      int i1 = i + (a == 0), j1 = j + (a == 1), k1 = k + (a == 2);
-      d += (f[c + s] * Geo<COORD>::face(P, a, i1, j1, k1) - f[c] * Geo<COORD>::face(P, a, i, j, k)) /
-           vol;
-    }
-    db = fabs(d);
-  }
-  block_commit(dtc, db, P.scal + S_NEXT_DT, P.scal + S_DIVB);
-}
-
-// ------------------------------------------------------------------- AB2
-
-// W_h = W + c (W - W_old), mags and mags_h from the faces, B_h on faces
-// (src/solver_func.c:385-449) over the whole ghost-extended grid
-template <typename R>
-__global__ void k_ab2(Params P, Work<R> w) {
-  if (stopped(P)) return;
-  const int cb = cur_buf(P);
-  const double* __restrict__ W = P.Wbuf[cb];
-  const double* __restrict__ Wo = P.Wbuf[1 - cb];
-  const double* __restrict__ B = P.Bbuf[cb];
-  const double* __restrict__ Bo = P.Bbuf[1 - cb];
-  R* __restrict__ Wh = w.Wh;
-  R* __restrict__ Ms = w.Ms;
-  R* __restrict__ Msh = w.Msh;
-  R* __restrict__ Bh = w.Bh;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
-  int k = blockIdx.z * blockDim.z + threadIdx.z;
-  if (i >= P.N[0] || j >= P.N[1] || k >= P.N[2]) return;
-  const double c = P.scal[S_CAB2];
-  long long x = lin(P, i, j, k);
-  bool ci = i < P.N[0] - 1, cj = j < P.N[1] - 1, ck = k < P.N[2] - 1;
-  if (ci && cj && ck) {
-#pragma unroll
-    for (int m = 0; m < 6; m++) {
-      double w = W[x + m * P.fs], wo = Wo[x + m * P.fs];
-      Wh[x + m * P.fs] = (R)(w + c * (w - wo));
-    }
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-      double ms = mags_at(P, B, a, i, j, k), mo = mags_at(P, Bo, a, i, j, k);
-      Ms[x + a * P.fs] = (R)ms;
-      Msh[x + a * P.fs] = (R)(ms + c * (ms - mo));
-    }
-  }
-#pragma unroll
-  for (int a = 0; a < 3; a++) {
-    bool ok = (a == 0 || ci) && (a == 1 || cj) && (a == 2 || ck);
-    if (ok) {
-      double b = B[x + a * P.fs], bo = Bo[x + a * P.fs];
-      Bh[x + a * P.fs] = (R)(b + c * (b - bo));
-    }
-  }
-}
-
-// ------------------------------------------------------------- edge EMF
-
 template <int AX>
 __device__ __forceinline__ long long sd(const Params& P) {
   return AX == 0 ? 1LL : (AX == 1 ? P.sj : P.sk);
@@ -228,23 +121,114 @@ __device__ __forceinline__ void line8(const T* __restrict__ a, long long s, R v[
 __device__ __forceinline__ double rsq(double x) { return rsqrt(x); }
 __device__ __forceinline__ float rsq(float x) { return rsqrtf(x); }
 
+// thread coordinates in a launch space
+struct Pos {
+  int x, y, z;
+};
+__device__ __forceinline__ Pos grid_pos() {
+  return {(int)(blockIdx.x * blockDim.x + threadIdx.x), (int)(blockIdx.y * blockDim.y + threadIdx.y),
+          (int)(blockIdx.z * blockDim.z + threadIdx.z)};
+}
+// batched launches: item = (member << 48) | (bx << 32) | (by << 16) | bz
+__device__ __forceinline__ Pos item_pos(unsigned long long it, int& member) {
+  member = (int)(it >> 48);
+  const int bx = (int)((it >> 32) & 0xffff), by = (int)((it >> 16) & 0xffff), bz = (int)(it & 0xffff);
+  return {(int)(bx * blockDim.x + threadIdx.x), (int)(by * blockDim.y + threadIdx.y),
+          (int)(bz * blockDim.z + threadIdx.z)};
+}
+
+// ---------------------------------------------------------- step control
+
+// open the step (src/solver_solve.c:103-107, src/solver_func.c:385-491):
+// dt from the running CFL minimum, time, AB2 coefficient; stop once the
+// previous step passed time_stop or the step budget is spent
+__device__ __forceinline__ void begin_body(const Params& P) {
+  double* s = P.scal;
+  if (s[S_STOP] != 0.0) return;
+  if (s[S_TIME] > s[S_TSTOP] || s[S_BUDGET] <= 0.0) {
+    s[S_STOP] = 1.0;
+    return;
+  }
+  s[S_BUDGET] = s[S_BUDGET] - 1.0;
+  const double dt = s[S_NEXT_DT];
+  if (!(dt > 0.0) || !isfinite(dt)) s[S_FLAGS] = 1.0;
+  s[S_DT] = dt;
+  s[S_TIME] = s[S_TIME] + dt;
+  s[S_CAB2] = 0.5 * dt / s[S_DT0];
+  s[S_DT0] = dt;
+  s[S_NEXT_DT] = DBL_MAX;
+  s[S_DIVB] = 0.0;
+  s[S_STEPS] = s[S_STEPS] + 1.0;
+}
+
+// close the step: the buffer written by this step becomes the current state
+__device__ __forceinline__ void end_body(const Params& P) {
+  if (P.scal[S_STOP] != 0.0) return;
+  P.scal[S_PAR] = P.scal[S_PAR] != 0.0 ? 0.0 : 1.0;
+}
+
+__device__ __forceinline__ void arm_body(const Params& P, double tstop, double budget) {
+  P.scal[S_TSTOP] = tstop;
+  P.scal[S_BUDGET] = budget;
+  P.scal[S_STOP] = 0.0;
+}
+
+// ------------------------------------------------------------------- AB2
+
+// W_h = W + c (W - W_old), mags and mags_h from the faces, B_h on faces
+// (src/solver_func.c:385-449) over the whole ghost-extended grid
+template <typename R>
+__device__ __forceinline__ void ab2_body(const Params& P, const Work<R>& w, Pos t) {
+  const int i = t.x, j = t.y, k = t.z;
+  if (i >= P.N[0] || j >= P.N[1] || k >= P.N[2]) return;
+  const int cb = cur_buf(P);
+  const double* __restrict__ W = P.Wbuf[cb];
+  const double* __restrict__ Wo = P.Wbuf[1 - cb];
+  const double* __restrict__ B = P.Bbuf[cb];
+  const double* __restrict__ Bo = P.Bbuf[1 - cb];
+  const double c = P.scal[S_CAB2];
+  const long long x = lin(P, i, j, k);
+  const size_t fs = P.fs;
+  const bool ci = i < P.N[0] - 1, cj = j < P.N[1] - 1, ck = k < P.N[2] - 1;
+  if (ci && cj && ck) {
+#pragma unroll
+    for (int m = 0; m < 6; m++) {
+      const double v = W[x + m * fs], vo = Wo[x + m * fs];
+      w.Wh[x + m * fs] = (R)(v + c * (v - vo));
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const double ms = mags_at(P, B, a, i, j, k), mo = mags_at(P, Bo, a, i, j, k);
+      w.Ms[x + a * fs] = (R)ms;
+      w.Msh[x + a * fs] = (R)(ms + c * (ms - mo));
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const bool ok = (a == 0 || ci) && (a == 1 || cj) && (a == 2 || ck);
+    if (ok) {
+      const double b = B[x + a * fs], bo = Bo[x + a * fs];
+      w.Bh[x + a * fs] = (R)(b + c * (b - bo));
+    }
+  }
+}
+
+// ------------------------------------------------------------- edge EMF
+
 // First centre-to-edge sweep of center2corner_{jk,ki,ij}
 // (src/solver_func.c:686-778): for edges along D, velocity components
 // p=(D+1)%3 and q=(D+2)%3 reconstructed along p (limiter on the step-start
 // velocity) and averaged.  Points: D active, p faces lo..hi+1, q all ghosts.
 template <typename R, int D>
-__global__ void __launch_bounds__(256) k_c2c(Params P, Work<R> wk) {
+__device__ __forceinline__ void c2c_body(const Params& P, const Work<R>& wk, Pos t) {
   constexpr int p = (D + 1) % 3, q = (D + 2) % 3;
-  if (stopped(P)) return;
-  int ijk[3] = {(int)(blockIdx.x * blockDim.x + threadIdx.x),
-                (int)(blockIdx.y * blockDim.y + threadIdx.y),
-                (int)(blockIdx.z * blockDim.z + threadIdx.z)};
+  const int ijk[3] = {t.x, t.y, t.z};
   int cnt[3], lo[3];
   lo[D] = NGH; cnt[D] = P.n[D];
   lo[p] = NGH; cnt[p] = P.n[p] + 1;
   lo[q] = 0;   cnt[q] = P.n[q] + 2 * NGH;
   if (ijk[0] >= cnt[0] || ijk[1] >= cnt[1] || ijk[2] >= cnt[2]) return;
-  int i = ijk[0] + lo[0], j = ijk[1] + lo[1], k = ijk[2] + lo[2];
+  const int i = ijk[0] + lo[0], j = ijk[1] + lo[1], k = ijk[2] + lo[2];
   const int f = p == 0 ? i : (p == 1 ? j : k);
   const long long x = lin(P, i, j, k), s = sd<p>(P);
   const size_t fs = P.fs;
@@ -258,7 +242,7 @@ __global__ void __launch_bounds__(256) k_c2c(Params P, Work<R> wk) {
     R v[8], lim[4], L, Rr;
     line8<R, R>(wk.Wh + (size_t)(V1 + comp) * fs + x, s, v);
 #pragma unroll
-    for (int t = 0; t < 4; t++) lim[t] = (R)W[(V1 + comp) * fs + (t - 2) * s];
+    for (int u = 0; u < 4; u++) lim[u] = (R)W[(V1 + comp) * fs + (u - 2) * s];
     recon_lr<R>(v, lim, Wt, a1, a2, L, Rr);
     wk.V[x + (size_t)(2 * D + cc) * fs] = R(0.5) * (L + Rr);
   }
@@ -267,12 +251,9 @@ __global__ void __launch_bounds__(256) k_c2c(Params P, Work<R> wk) {
 // Second sweep, face-field reconstruction and the edge EMF
 // (src/solver_func.c:779-902) for edges along D: D active, p and q faces.
 template <typename R, int D>
-__global__ void __launch_bounds__(256) k_emf(Params P, Work<R> wk) {
+__device__ __forceinline__ void emf_body(const Params& P, const Work<R>& wk, Pos t) {
   constexpr int p = (D + 1) % 3, q = (D + 2) % 3;
-  if (stopped(P)) return;
-  int ijk[3] = {(int)(blockIdx.x * blockDim.x + threadIdx.x),
-                (int)(blockIdx.y * blockDim.y + threadIdx.y),
-                (int)(blockIdx.z * blockDim.z + threadIdx.z)};
+  const int ijk[3] = {t.x, t.y, t.z};
   int cnt[3];
   cnt[D] = P.n[D];
   cnt[p] = P.n[p] + 1;
@@ -293,7 +274,7 @@ __global__ void __launch_bounds__(256) k_emf(Params P, Work<R> wk) {
       R v[8], lim[4], L, Rr;
       line8<R, R>(wk.V + (size_t)(2 * D + cc) * fs + x, sq, v);
 #pragma unroll
-      for (int t = 0; t < 4; t++) lim[t] = v[t + 2];
+      for (int u = 0; u < 4; u++) lim[u] = v[u + 2];
       recon_lr<R>(v, lim, Wt, a1, a2, L, Rr);
       vav[cc] = R(0.5) * (L + Rr);
     }
@@ -301,7 +282,7 @@ __global__ void __launch_bounds__(256) k_emf(Params P, Work<R> wk) {
     R v[8], lim[4];
     line8<R, R>(wk.Bh + (size_t)p * fs + x, sq, v);
 #pragma unroll
-    for (int t = 0; t < 4; t++) lim[t] = (R)B[p * fs + (t - 2) * sq];
+    for (int u = 0; u < 4; u++) lim[u] = (R)B[p * fs + (u - 2) * sq];
     recon_lr<R>(v, lim, Wt, a1, a2, bpl, bpr);
   }
   {
@@ -311,7 +292,7 @@ __global__ void __launch_bounds__(256) k_emf(Params P, Work<R> wk) {
     R v[8], lim[4];
     line8<R, R>(wk.Bh + (size_t)q * fs + x, sp, v);
 #pragma unroll
-    for (int t = 0; t < 4; t++) lim[t] = (R)B[q * fs + (t - 2) * sp];
+    for (int u = 0; u < 4; u++) lim[u] = (R)B[q * fs + (u - 2) * sp];
     recon_lr<R>(v, lim, Wt, a1, a2, bql, bqr);
   }
   const R bp = R(0.5) * (bpl + bpr), bq = R(0.5) * (bql + bqr);
@@ -319,8 +300,8 @@ __global__ void __launch_bounds__(256) k_emf(Params P, Work<R> wk) {
   R e = -(vp * bq - vq * bp);
   const R* rh = wk.Wh + x;  // density slot
   // the reference sums the four densities around the edge in (i,j,k) order
-  R rho4 = D == 1 ? rh[-sq - sp] + rh[-sq] + rh[-sp] + rh[0]
-                  : rh[-sp - sq] + rh[-sp] + rh[-sq] + rh[0];
+  const R rho4 = D == 1 ? rh[-sq - sp] + rh[-sq] + rh[-sp] + rh[0]
+                        : rh[-sp - sq] + rh[-sp] + rh[-sq] + rh[0];
   const R ca = (R)P.ca;
   R vz = sqrt((bp * bp + bq * bq) / (R(0.25) * rho4));
   vz = vz * ca * rsq(vz * vz + ca * ca) + sqrt(vp * vp + vq * vq);
@@ -334,11 +315,8 @@ __global__ void __launch_bounds__(256) k_emf(Params P, Work<R> wk) {
 // (src/solver_func.c:934-1529).  F[9] = mass, 3 momenta, energy, entropy,
 // 3 stress components.
 template <typename R, int D>
-__global__ void __launch_bounds__(256, 2) k_flux(Params P, Work<R> wk) {
-  if (stopped(P)) return;
-  const int i = NGH + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = NGH + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = NGH + blockIdx.z * blockDim.z + threadIdx.z;
+__device__ __forceinline__ void flux_body(const Params& P, const Work<R>& wk, Pos t) {
+  const int i = NGH + t.x, j = NGH + t.y, k = NGH + t.z;
   if (i >= NGH + P.n[0] + (D == 0) || j >= NGH + P.n[1] + (D == 1) ||
       k >= NGH + P.n[2] + (D == 2))
     return;
@@ -356,7 +334,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(Params P, Work<R> wk) {
     R v[8], lim[4];
     line8<R, R>(wk.Wh + (size_t)m * fs + x, s, v);
 #pragma unroll
-    for (int t = 0; t < 4; t++) lim[t] = (R)W[m * fs + (t - 2) * s];
+    for (int u = 0; u < 4; u++) lim[u] = (R)W[m * fs + (u - 2) * s];
     recon_lr<R>(v, lim, Wt, a1, a2, L[m], Rt[m]);
   }
 #pragma unroll
@@ -365,7 +343,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(Params P, Work<R> wk) {
     line8<R, R>(wk.Msh + (size_t)a * fs + x, s, v);
     const R* ms = wk.Ms + (size_t)a * fs + x;
 #pragma unroll
-    for (int t = 0; t < 4; t++) lim[t] = ms[(t - 2) * s];
+    for (int u = 0; u < 4; u++) lim[u] = ms[(u - 2) * s];
     recon_lr<R>(v, lim, Wt, a1, a2, mL[a], mR[a]);
   }
   const R gm = (R)P.gamma, gm1 = (R)P.gm1, ca = (R)P.ca, ca2 = (R)P.ca2;
@@ -399,9 +377,9 @@ __global__ void __launch_bounds__(256, 2) k_flux(Params P, Work<R> wk) {
   o[0] = R(0.5) * (mol[D] + mor[D] - vf * (rr - rl));
 #pragma unroll
   for (int a = 0; a < 3; a++) {
-    R t = mol[a] * vnl + mor[a] * vnr - vf * (mor[a] - mol[a]);
-    if (a == D) t = mol[a] * vnl + pl + mor[a] * vnr + pr - vf * (mor[a] - mol[a]);
-    o[(1 + a) * fs] = R(0.5) * t;
+    R u = mol[a] * vnl + mor[a] * vnr - vf * (mor[a] - mol[a]);
+    if (a == D) u = mol[a] * vnl + pl + mor[a] * vnr + pr - vf * (mor[a] - mol[a]);
+    o[(1 + a) * fs] = R(0.5) * u;
   }
   o[4 * fs] = R(0.5) * (el * vnl + pl * vnl + er * vnr + pr * vnr - vf * (er - el));
   o[5 * fs] = R(0.5) * (Sl * vnl + Sr * vnr - vfe * (Sr - Sl));
@@ -441,178 +419,195 @@ __device__ __forceinline__ double ct_face(const Params& P, const double* __restr
   return B[x + A * fs] - dt * (cq - cp) / Geo<COORD>::face(P, A, i, j, k);
 }
 
+// one active cell: returns its CFL dt and |div B| of the new state
 template <int COORD, typename R>
-__global__ void __launch_bounds__(256) k_update(Params P, Work<R> wk) {
-  if (stopped(P)) return;
-  const int i = NGH + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = NGH + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = NGH + blockIdx.z * blockDim.z + threadIdx.z;
-  double dtc = DBL_MAX, dbmax = 0.0;
-  const bool inside = i < NGH + P.n[0] && j < NGH + P.n[1] && k < NGH + P.n[2];
-  if (inside) {
-    const size_t fs = P.fs;
-    const double dt = P.scal[S_DT];
-    const int cb = cur_buf(P);
-    const double* __restrict__ W = P.Wbuf[cb];
-    const double* __restrict__ B = P.Bbuf[cb];
-    double* __restrict__ Wn = P.Wbuf[1 - cb];
-    double* __restrict__ Bn = P.Bbuf[1 - cb];
-    const R* __restrict__ F = wk.F;
-    const R* __restrict__ E = wk.E;
-    const long long x = lin(P, i, j, k);
-    const double vol = Geo<COORD>::vol(P, i, j, k);
-    const double ivol = 1.0 / vol;
-    double du[6], dm[3], fl[3], fu[3];
+__device__ __forceinline__ void update_body(const Params& P, const Work<R>& wk, Pos t,
+                                            double& dtc, double& dbmax) {
+  const int i = NGH + t.x, j = NGH + t.y, k = NGH + t.z;
+  if (i >= NGH + P.n[0] || j >= NGH + P.n[1] || k >= NGH + P.n[2]) return;
+  const size_t fs = P.fs;
+  const double dt = P.scal[S_DT];
+  const int cb = cur_buf(P);
+  const double* __restrict__ W = P.Wbuf[cb];
+  const double* __restrict__ B = P.Bbuf[cb];
+  double* __restrict__ Wn = P.Wbuf[1 - cb];
+  double* __restrict__ Bn = P.Bbuf[1 - cb];
+  const R* __restrict__ F = wk.F;
+  const R* __restrict__ E = wk.E;
+  const long long x = lin(P, i, j, k);
+  const double vol = Geo<COORD>::vol(P, i, j, k);
+  const double ivol = 1.0 / vol;
+  double du[6], dm[3], fl[3], fu[3];
 #pragma unroll
-    for (int d = 0; d < 3; d++) {
-      const long long s = stride(P, d);
-      const int i1 = i + (d == 0), j1 = j + (d == 1), k1 = k + (d == 2);
-      fl[d] = Geo<COORD>::face(P, d, i, j, k);
-      fu[d] = Geo<COORD>::face(P, d, i1, j1, k1);
-      const R* Fd = F + (size_t)(9 * d) * fs + x;
+  for (int d = 0; d < 3; d++) {
+    const long long s = stride(P, d);
+    const int i1 = i + (d == 0), j1 = j + (d == 1), k1 = k + (d == 2);
+    fl[d] = Geo<COORD>::face(P, d, i, j, k);
+    fu[d] = Geo<COORD>::face(P, d, i1, j1, k1);
+    const R* Fd = F + (size_t)(9 * d) * fs + x;
 #pragma unroll
-      for (int m = 0; m < 6; m++) {
-        double v = ((double)Fd[s + m * fs] * fu[d] - (double)Fd[m * fs] * fl[d]) * ivol;
-        du[m] = d == 0 ? v : du[m] + v;
-      }
-#pragma unroll
-      for (int a = 0; a < 3; a++) {
-        double v = ((double)Fd[s + (6 + a) * fs] * fu[d] - (double)Fd[(6 + a) * fs] * fl[d]) * ivol;
-        dm[a] = d == 0 ? v : dm[a] + v;
-      }
+    for (int m = 0; m < 6; m++) {
+      double v = ((double)Fd[s + m * fs] * fu[d] - (double)Fd[m * fs] * fl[d]) * ivol;
+      du[m] = d == 0 ? v : du[m] + v;
     }
-    // spherical geometric sources (src/spherical/spherical_general.c:605-681)
-    double sh[3] = {0.0, 0.0, 0.0}, sb[3] = {0.0, 0.0, 0.0};
-    if (COORD == 2) {
-      const long long si = 1, sjj = P.sj;
-      const double fi0 = fl[0], fi1 = fu[0], fj0 = fl[1], fj1 = fu[1];
-      const double dr = tb(P, 0, T_DX, i), rc = tb(P, 0, T_G3, i);
-      const R* Wh = wk.Wh + x;
-      const double ph = Wh[PR * fs], rh = Wh[RHO * fs], v2h = Wh[V2 * fs], v3h = Wh[V3 * fs];
-      const double m22 = ph + rh * v2h * v2h, m33 = ph + rh * v3h * v3h;
-      const R* Fi = F + x;
-      const R* Fj = F + (size_t)9 * fs + x;
-      const double geo = dr / rc / 2.0 * ivol;
-      sh[0] = 0.5 * (m22 + m33) * (fi1 - fi0) * ivol;
-      sh[1] = -((double)Fi[2 * fs] * fi0 + (double)Fi[si + 2 * fs] * fi1) * geo + (fj1 - fj0) * ivol * m33;
-      sh[2] = -((double)Fi[3 * fs] * fi0 + (double)Fi[si + 3 * fs] * fi1) * geo;
-      const double sr = tb(P, 1, T_G3, j) / tb(P, 1, T_G4, j) * ivol;
-      sh[2] += -((double)Fj[3 * fs] * fj0 + (double)Fj[sjj + 3 * fs] * fj1) * sr;
-      const R* Msh = wk.Msh + x;
-      const double b1 = Msh[0], b2 = Msh[fs], b3 = Msh[2 * fs];
-      const double bsq = b1 * b1 + b2 * b2 + b3 * b3;
-      const double n22 = 0.5 * bsq - b2 * b2, n33 = 0.5 * bsq - b3 * b3;
-      sb[0] = 0.5 * (n22 + n33) * (fi1 - fi0) * ivol;
-      sb[1] = -((double)Fi[7 * fs] * fi0 + (double)Fi[si + 7 * fs] * fi1) * geo + (fj1 - fj0) * ivol * n33;
-      sb[2] = -((double)Fi[8 * fs] * fi0 + (double)Fi[si + 8 * fs] * fi1) * geo;
-      sb[2] += -((double)Fj[8 * fs] * fj0 + (double)Fj[sjj + 8 * fs] * fj1) * sr;
-    }
-    // new face fields: this cell's lower faces and its upper faces
-    double bl[3], bu[3];
-    bl[0] = ct_face<COORD, 0, R>(P, B, E, i, j, k, dt);
-    bl[1] = ct_face<COORD, 1, R>(P, B, E, i, j, k, dt);
-    bl[2] = ct_face<COORD, 2, R>(P, B, E, i, j, k, dt);
-    bu[0] = ct_face<COORD, 0, R>(P, B, E, i + 1, j, k, dt);
-    bu[1] = ct_face<COORD, 1, R>(P, B, E, i, j + 1, k, dt);
-    bu[2] = ct_face<COORD, 2, R>(P, B, E, i, j, k + 1, dt);
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-      Bn[x + a * fs] = bl[a];
-      const int pos = a == 0 ? i : (a == 1 ? j : k);
-      if (pos == NGH + P.n[a] - 1) Bn[x + stride(P, a) + a * fs] = bu[a];
+      double v = ((double)Fd[s + (6 + a) * fs] * fu[d] - (double)Fd[(6 + a) * fs] * fl[d]) * ivol;
+      dm[a] = d == 0 ? v : dm[a] + v;
     }
-    // U^n from W^n (src/solver_func.c:356-382)
-    const double gm1 = P.gm1;
-    const double r0 = W[x], u0 = W[x + fs], v0 = W[x + 2 * fs], w0 = W[x + 3 * fs],
-                 p0 = W[x + 4 * fs], ps0 = W[x + 5 * fs];
-    double U[6];
-    U[0] = r0;
-    U[1] = r0 * u0;
-    U[2] = r0 * v0;
-    U[3] = r0 * w0;
-    U[4] = 0.5 * r0 * (u0 * u0 + v0 * v0 + w0 * w0) + p0 * P.inv_gm1;
-    U[5] = (ps0 == 0.0 && r0 > 0.0) ? ps0 : ps0 / pow(r0, gm1);
-    const double U0[3] = {U[1], U[2], U[3]};
-    // conservative update and cons->prim (src/solver_solve.c:326-377)
-    U[0] -= dt * du[0];
-#pragma unroll
-    for (int a = 0; a < 3; a++) U[1 + a] = U[1 + a] - dt * du[1 + a] + dt * sh[a];
-    U[4] -= dt * du[4];
-    U[5] -= dt * du[5];
-    double rho = U[0];
-    const double irho = 1.0 / U[0];
-    double vv[3] = {U[1] * irho, U[2] * irho, U[3] * irho};
-    double p = (U[4] - 0.5 * (vv[0] * vv[0] + vv[1] * vv[1] + vv[2] * vv[2]) * rho) * gm1;
-    const double pS = (U[5] == 0.0 && U[0] > 0.0) ? U[5] : U[5] * pow(U[0], gm1);
-    // positivity floors (src/solver_func.c:2117-2135)
-    if (rho < P.rho_floor) {
-      rho = P.rho_floor;
-      p = P.p_floor;
-    }
-    if (p < P.p_floor) p = P.p_floor;
-    // mags^{n+1}, time-centred field, Alfven/Boris correction
-    // (src/solver_solve.c:385-484)
-    double mt[3], mn[3];
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-      const int idx = a == 0 ? i : (a == 1 ? j : k);
-      mn[a] = bl[a] * tb(P, a, T_MA, idx) + bu[a] * tb(P, a, T_MB, idx);
-      mt[a] = 0.5 * (mn[a] + mags_at(P, B, a, i, j, k));
-    }
-    const double bsq = mt[0] * mt[0] + mt[1] * mt[1] + mt[2] * mt[2];
-    const double alf = bsq / rho / P.ca2;
-    const double perp = 1.0 / (1.0 + alf);
-    const double drho = -dt * du[0];
-    const double dva = alf * drho;
-    double tv[3];
-#pragma unroll
-    for (int a = 0; a < 3; a++) tv[a] = alf * (-dt * du[1 + a] + dt * sh[a] - drho * W[x + (1 + a) * fs]);
-    double bdv = mt[0] * tv[0] + mt[1] * tv[1] + mt[2] * tv[2];
-    bdv = bdv / (bsq + 1e-10);
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-      const double mom = U0[a] + perp * ((-dt * du[1 + a] + dt * sh[a]) + (-dt * dm[a] + dt * sb[a]) +
-                                         dva * W[x + (1 + a) * fs] + mt[a] * bdv);
-      vv[a] = mom * irho;
-    }
-    Wn[x] = rho;
-    Wn[x + fs] = vv[0];
-    Wn[x + 2 * fs] = vv[1];
-    Wn[x + 3 * fs] = vv[2];
-    Wn[x + 4 * fs] = p;
-    Wn[x + 5 * fs] = pS;
-    // CFL dt of the new state (magtot = mags^{n+1}) and max|div B^{n+1}|
-    dtc = cfl_cell<COORD>(P, i, j, k, rho, vv[0], vv[1], vv[2], p, mn[0], mn[1], mn[2]);
-    const double dvb = (bu[0] * fu[0] - bl[0] * fl[0]) * ivol + (bu[1] * fu[1] - bl[1] * fl[1]) * ivol +
-                       (bu[2] * fu[2] - bl[2] * fl[2]) * ivol;
-    dbmax = fabs(dvb);
-    if (!(dtc > 0.0) || !isfinite(p) || !isfinite(rho) || !isfinite(vv[0] + vv[1] + vv[2]))
-      P.scal[S_FLAGS] = 1.0;
   }
-  block_commit(dtc, dbmax, P.scal + S_NEXT_DT, P.scal + S_DIVB);
+  // spherical geometric sources (src/spherical/spherical_general.c:605-681)
+  double sh[3] = {0.0, 0.0, 0.0}, sb[3] = {0.0, 0.0, 0.0};
+  if (COORD == 2) {
+    const long long si = 1, sjj = P.sj;
+    const double fi0 = fl[0], fi1 = fu[0], fj0 = fl[1], fj1 = fu[1];
+    const double dr = tb(P, 0, T_DX, i), rc = tb(P, 0, T_G3, i);
+    const R* Wh = wk.Wh + x;
+    const double ph = Wh[PR * fs], rh = Wh[RHO * fs], v2h = Wh[V2 * fs], v3h = Wh[V3 * fs];
+    const double m22 = ph + rh * v2h * v2h, m33 = ph + rh * v3h * v3h;
+    const R* Fi = F + x;
+    const R* Fj = F + (size_t)9 * fs + x;
+    const double geo = dr / rc / 2.0 * ivol;
+    sh[0] = 0.5 * (m22 + m33) * (fi1 - fi0) * ivol;
+    sh[1] = -((double)Fi[2 * fs] * fi0 + (double)Fi[si + 2 * fs] * fi1) * geo + (fj1 - fj0) * ivol * m33;
+    sh[2] = -((double)Fi[3 * fs] * fi0 + (double)Fi[si + 3 * fs] * fi1) * geo;
+    const double sr = tb(P, 1, T_G3, j) / tb(P, 1, T_G4, j) * ivol;
+    sh[2] += -((double)Fj[3 * fs] * fj0 + (double)Fj[sjj + 3 * fs] * fj1) * sr;
+    const R* Msh = wk.Msh + x;
+    const double b1 = Msh[0], b2 = Msh[fs], b3 = Msh[2 * fs];
+    const double bsq = b1 * b1 + b2 * b2 + b3 * b3;
+    const double n22 = 0.5 * bsq - b2 * b2, n33 = 0.5 * bsq - b3 * b3;
+    sb[0] = 0.5 * (n22 + n33) * (fi1 - fi0) * ivol;
+    sb[1] = -((double)Fi[7 * fs] * fi0 + (double)Fi[si + 7 * fs] * fi1) * geo + (fj1 - fj0) * ivol * n33;
+    sb[2] = -((double)Fi[8 * fs] * fi0 + (double)Fi[si + 8 * fs] * fi1) * geo;
+    sb[2] += -((double)Fj[8 * fs] * fj0 + (double)Fj[sjj + 8 * fs] * fj1) * sr;
+  }
+  // new face fields: this cell's lower faces and its upper faces
+  double bl[3], bu[3];
+  bl[0] = ct_face<COORD, 0, R>(P, B, E, i, j, k, dt);
+  bl[1] = ct_face<COORD, 1, R>(P, B, E, i, j, k, dt);
+  bl[2] = ct_face<COORD, 2, R>(P, B, E, i, j, k, dt);
+  bu[0] = ct_face<COORD, 0, R>(P, B, E, i + 1, j, k, dt);
+  bu[1] = ct_face<COORD, 1, R>(P, B, E, i, j + 1, k, dt);
+  bu[2] = ct_face<COORD, 2, R>(P, B, E, i, j, k + 1, dt);
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    Bn[x + a * fs] = bl[a];
+    const int pos = a == 0 ? i : (a == 1 ? j : k);
+    if (pos == NGH + P.n[a] - 1) Bn[x + stride(P, a) + a * fs] = bu[a];
+  }
+  // U^n from W^n (src/solver_func.c:356-382)
+  const double gm1 = P.gm1;
+  const double r0 = W[x], u0 = W[x + fs], v0 = W[x + 2 * fs], w0 = W[x + 3 * fs],
+               p0 = W[x + 4 * fs], ps0 = W[x + 5 * fs];
+  double U[6];
+  U[0] = r0;
+  U[1] = r0 * u0;
+  U[2] = r0 * v0;
+  U[3] = r0 * w0;
+  U[4] = 0.5 * r0 * (u0 * u0 + v0 * v0 + w0 * w0) + p0 * P.inv_gm1;
+  U[5] = (ps0 == 0.0 && r0 > 0.0) ? ps0 : ps0 / pow(r0, gm1);
+  const double U0[3] = {U[1], U[2], U[3]};
+  // conservative update and cons->prim (src/solver_solve.c:326-377)
+  U[0] -= dt * du[0];
+#pragma unroll
+  for (int a = 0; a < 3; a++) U[1 + a] = U[1 + a] - dt * du[1 + a] + dt * sh[a];
+  U[4] -= dt * du[4];
+  U[5] -= dt * du[5];
+  double rho = U[0];
+  const double irho = 1.0 / U[0];
+  double vv[3] = {U[1] * irho, U[2] * irho, U[3] * irho};
+  double p = (U[4] - 0.5 * (vv[0] * vv[0] + vv[1] * vv[1] + vv[2] * vv[2]) * rho) * gm1;
+  const double pS = (U[5] == 0.0 && U[0] > 0.0) ? U[5] : U[5] * pow(U[0], gm1);
+  // positivity floors (src/solver_func.c:2117-2135)
+  if (rho < P.rho_floor) {
+    rho = P.rho_floor;
+    p = P.p_floor;
+  }
+  if (p < P.p_floor) p = P.p_floor;
+  // mags^{n+1}, time-centred field, Alfven/Boris correction
+  // (src/solver_solve.c:385-484)
+  double mt[3], mn[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const int idx = a == 0 ? i : (a == 1 ? j : k);
+    mn[a] = bl[a] * tb(P, a, T_MA, idx) + bu[a] * tb(P, a, T_MB, idx);
+    mt[a] = 0.5 * (mn[a] + mags_at(P, B, a, i, j, k));
+  }
+  const double bsq = mt[0] * mt[0] + mt[1] * mt[1] + mt[2] * mt[2];
+  const double alf = bsq / rho / P.ca2;
+  const double perp = 1.0 / (1.0 + alf);
+  const double drho = -dt * du[0];
+  const double dva = alf * drho;
+  double tv[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) tv[a] = alf * (-dt * du[1 + a] + dt * sh[a] - drho * W[x + (1 + a) * fs]);
+  double bdv = mt[0] * tv[0] + mt[1] * tv[1] + mt[2] * tv[2];
+  bdv = bdv / (bsq + 1e-10);
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const double mom = U0[a] + perp * ((-dt * du[1 + a] + dt * sh[a]) + (-dt * dm[a] + dt * sb[a]) +
+                                       dva * W[x + (1 + a) * fs] + mt[a] * bdv);
+    vv[a] = mom * irho;
+  }
+  Wn[x] = rho;
+  Wn[x + fs] = vv[0];
+  Wn[x + 2 * fs] = vv[1];
+  Wn[x + 3 * fs] = vv[2];
+  Wn[x + 4 * fs] = p;
+  Wn[x + 5 * fs] = pS;
+  // CFL dt of the new state (magtot = mags^{n+1}) and max|div B^{n+1}|
+  dtc = cfl_cell<COORD>(P, i, j, k, rho, vv[0], vv[1], vv[2], p, mn[0], mn[1], mn[2]);
+  const double dvb = (bu[0] * fu[0] - bl[0] * fl[0]) * ivol + (bu[1] * fu[1] - bl[1] * fl[1]) * ivol +
+                     (bu[2] * fu[2] - bl[2] * fl[2]) * ivol;
+  dbmax = fabs(dvb);
+  if (!(dtc > 0.0) || !isfinite(p) || !isfinite(rho) || !isfinite(vv[0] + vv[1] + vv[2]))
+    P.scal[S_FLAGS] = 1.0;
+}
+
+// CFL dt and |div B| of one cell of the current state (prepare)
+template <int COORD>
+__device__ __forceinline__ void dt_body(const Params& P, Pos t, double& dtc, double& db) {
+  const int i = NGH + t.x, j = NGH + t.y, k = NGH + t.z;
+  if (i >= NGH + P.n[0] || j >= NGH + P.n[1] || k >= NGH + P.n[2]) return;
+  const double* __restrict__ W = P.Wbuf[cur_buf(P)];
+  const double* __restrict__ B = P.Bbuf[cur_buf(P)];
+  const long long c = lin(P, i, j, k);
+  const double b1 = mags_at(P, B, 0, i, j, k), b2 = mags_at(P, B, 1, i, j, k),
+               b3 = mags_at(P, B, 2, i, j, k);
+  dtc = cfl_cell<COORD>(P, i, j, k, W[c], W[c + P.fs], W[c + 2 * P.fs], W[c + 3 * P.fs],
+                        W[c + 4 * P.fs], b1, b2, b3);
+  const double vol = Geo<COORD>::vol(P, i, j, k);
+  double d = 0.0;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const double* f = B + (size_t)a * P.fs;
+    const long long s = stride(P, a);
+    const int i1 = i + (a == 0), j1 = j + (a == 1), k1 = k + (a == 2);
+    d += (f[c + s] * Geo<COORD>::face(P, a, i1, j1, k1) - f[c] * Geo<COORD>::face(P, a, i, j, k)) / vol;
+  }
+  db = fabs(d);
 }
 
 // ---------------------------------------------------------------- ghosts
 
 // Periodic wrap of one axis for all 9 state fields (src/boundary_exchange.c,
 // index sets of src/setup_mpi.c:62-253), over the full transverse extent.
-__global__ void k_wrap(Params P, int axis, int which) {
-  if (stopped(P)) return;
+// Space: (N[oa], N[ob], 2*NGH); sources (active layers) and destinations
+// (ghost layers) are disjoint for n >= NGH, so both sides go in one launch.
+__device__ __forceinline__ void wrap_body(const Params& P, int axis, int which, Pos t) {
+  const int oa = (axis + 1) % 3, ob = (axis + 2) % 3;
+  if (t.x >= P.N[oa] || t.y >= P.N[ob] || t.z >= 2 * NGH) return;
   const int bsel = which ? cur_buf(P) : 1 - cur_buf(P);
   double* __restrict__ W = P.Wbuf[bsel];
   double* __restrict__ B = P.Bbuf[bsel];
-  int oa = (axis + 1) % 3, ob = (axis + 2) % 3;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;  // transverse index a
-  int u = blockIdx.y * blockDim.y + threadIdx.y;  // transverse index b
-  int g = blockIdx.z;                             // 0..2*NGH-1
-  if (t >= P.N[oa] || u >= P.N[ob]) return;
-  int N = P.N[axis];
-  int side = g / NGH, l = g % NGH;
+  const int N = P.N[axis];
+  const int side = t.z / NGH, l = t.z % NGH;
   int ijk[3];
-  ijk[oa] = t;
-  ijk[ob] = u;
+  ijk[oa] = t.x;
+  ijk[ob] = t.y;
   for (int f = 0; f < 9; f++) {
-    int onface = (f >= 6 && f - 6 == axis) ? 1 : 0;
+    const int onface = (f >= 6 && f - 6 == axis) ? 1 : 0;
     double* a = f < 6 ? W + (size_t)f * P.fs : B + (size_t)(f - 6) * P.fs;
     int src, dst;
     if (side == 0) {  // high ghosts <- low active
@@ -623,7 +618,7 @@ __global__ void k_wrap(Params P, int axis, int which) {
       dst = l;
     }
     ijk[axis] = src;
-    double v = a[lin(P, ijk[0], ijk[1], ijk[2])];
+    const double v = a[lin(P, ijk[0], ijk[1], ijk[2])];
     ijk[axis] = dst;
     a[lin(P, ijk[0], ijk[1], ijk[2])] = v;
   }
@@ -631,29 +626,26 @@ __global__ void k_wrap(Params P, int axis, int which) {
 
 // One face of the ghost-fill library (src/boundary_conditions.c): the 6 gas
 // primitives with kind `kind` (gas_bc_*) and the 3 face fields with kind
-// `gkind` (gem_bc_*); 0 skips that group.
-__global__ void k_bcface(Params P, int axis, int side, int kind, int gkind, int which) {
-  if (stopped(P)) return;
+// `gkind` (gem_bc_*); 0 skips that group.  Space: (N[oa], N[ob], NGH).
+__device__ __forceinline__ void bcface_body(const Params& P, int axis, int side, int kind,
+                                            int gkind, int which, Pos t) {
+  const int oa = (axis + 1) % 3, ob = (axis + 2) % 3;
+  if (t.x >= P.N[oa] || t.y >= P.N[ob] || t.z >= NGH) return;
   const int bsel = which ? cur_buf(P) : 1 - cur_buf(P);
   double* __restrict__ W = P.Wbuf[bsel];
   double* __restrict__ B = P.Bbuf[bsel];
-  int oa = (axis + 1) % 3, ob = (axis + 2) % 3;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  int u = blockIdx.y * blockDim.y + threadIdx.y;
-  int l = blockIdx.z;
-  if (t >= P.N[oa] || u >= P.N[ob]) return;
-  int N = P.N[axis];
+  const int N = P.N[axis], l = t.z;
   int ijk[3];
-  ijk[oa] = t;
-  ijk[ob] = u;
+  ijk[oa] = t.x;
+  ijk[ob] = t.y;
   for (int f = 0; f < 9; f++) {
-    bool gas = f < 6;
-    int kd = gas ? kind : gkind;
+    const bool gas = f < 6;
+    const int kd = gas ? kind : gkind;
     if (kd == 0 || kd == 'n' || kd == 'p') continue;
     if (!gas && kd == 'r') continue;  // gem_bc_reflective_* are empty
-    int onface = (!gas && f - 6 == axis) ? 1 : 0;
+    const int onface = (!gas && f - 6 == axis) ? 1 : 0;
     double* a = gas ? W + (size_t)f * P.fs : B + (size_t)(f - 6) * P.fs;
-    int dst = side == 0 ? l : N - 1 - NGH + l + onface;
+    const int dst = side == 0 ? l : N - 1 - NGH + l + onface;
     double v;
     if (kd == 'f') {
       if (gas) {
@@ -677,43 +669,179 @@ __global__ void k_bcface(Params P, int axis, int side, int kind, int gkind, int 
   }
 }
 
+// ------------------------------------------------- single-instance kernels
+
+__global__ void k_begin(Params P) { begin_body(P); }
+__global__ void k_end(Params P) { end_body(P); }
+__global__ void k_arm(Params P, double tstop, double budget) { arm_body(P, tstop, budget); }
+
+template <int COORD>
+__global__ void k_dt(Params P) {
+  double dtc = DBL_MAX, db = 0.0;
+  dt_body<COORD>(P, grid_pos(), dtc, db);
+  block_commit(dtc, db, P.scal + S_NEXT_DT, P.scal + S_DIVB);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_ab2(Params P, Work<R> w) {
+  if (stopped(P)) return;
+  ab2_body<R>(P, w, grid_pos());
+}
+template <typename R, int D>
+__global__ void __launch_bounds__(256) k_c2c(Params P, Work<R> w) {
+  if (stopped(P)) return;
+  c2c_body<R, D>(P, w, grid_pos());
+}
+template <typename R, int D>
+__global__ void __launch_bounds__(256) k_emf(Params P, Work<R> w) {
+  if (stopped(P)) return;
+  emf_body<R, D>(P, w, grid_pos());
+}
+template <typename R, int D>
+__global__ void __launch_bounds__(256, 2) k_flux(Params P, Work<R> w) {
+  if (stopped(P)) return;
+  flux_body<R, D>(P, w, grid_pos());
+}
+template <int COORD, typename R>
+__global__ void __launch_bounds__(256) k_update(Params P, Work<R> w) {
+  if (stopped(P)) return;
+  double dtc = DBL_MAX, db = 0.0;
+  update_body<COORD, R>(P, w, grid_pos(), dtc, db);
+  block_commit(dtc, db, P.scal + S_NEXT_DT, P.scal + S_DIVB);
+}
+__global__ void k_wrap(Params P, int axis, int which) {
+  if (stopped(P)) return;
+  wrap_body(P, axis, which, grid_pos());
+}
+__global__ void k_bcface(Params P, int axis, int side, int kind, int gkind, int which) {
+  if (stopped(P)) return;
+  bcface_body(P, axis, side, kind, gkind, which, grid_pos());
+}
+
+// -------------------------------------------------------- batched kernels
+// Each block handles one (member, block) item of a work list built on the
+// host; members are independent grids with their own scalars.
+
+template <typename R>
+__global__ void kb_begin(const Member<R>* __restrict__ m, int n) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) begin_body(m[t].P);
+}
+template <typename R>
+__global__ void kb_end(const Member<R>* __restrict__ m, int n) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) end_body(m[t].P);
+}
+template <typename R>
+__global__ void kb_arm(const Member<R>* __restrict__ m, int n, const int* __restrict__ steps) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) arm_body(m[t].P, 1e300, (double)steps[t]);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) kb_ab2(const Member<R>* __restrict__ m,
+                                              const unsigned long long* __restrict__ items) {
+  int mi;
+  const Pos t = item_pos(items[blockIdx.x], mi);
+  const Member<R>& M = m[mi];
+  if (stopped(M.P)) return;
+  ab2_body<R>(M.P, M.w, t);
+}
+template <typename R, int D>
+__global__ void __launch_bounds__(256) kb_c2c(const Member<R>* __restrict__ m,
+                                              const unsigned long long* __restrict__ items) {
+  int mi;
+  const Pos t = item_pos(items[blockIdx.x], mi);
+  const Member<R>& M = m[mi];
+  if (stopped(M.P)) return;
+  c2c_body<R, D>(M.P, M.w, t);
+}
+template <typename R, int D>
+__global__ void __launch_bounds__(256) kb_emf(const Member<R>* __restrict__ m,
+                                              const unsigned long long* __restrict__ items) {
+  int mi;
+  const Pos t = item_pos(items[blockIdx.x], mi);
+  const Member<R>& M = m[mi];
+  if (stopped(M.P)) return;
+  emf_body<R, D>(M.P, M.w, t);
+}
+template <typename R, int D>
+__global__ void __launch_bounds__(256, 2) kb_flux(const Member<R>* __restrict__ m,
+                                                  const unsigned long long* __restrict__ items) {
+  int mi;
+  const Pos t = item_pos(items[blockIdx.x], mi);
+  const Member<R>& M = m[mi];
+  if (stopped(M.P)) return;
+  flux_body<R, D>(M.P, M.w, t);
+}
+template <typename R>
+__global__ void __launch_bounds__(256) kb_update(const Member<R>* __restrict__ m,
+                                                 const unsigned long long* __restrict__ items) {
+  int mi;
+  const Pos t = item_pos(items[blockIdx.x], mi);
+  const Member<R>& M = m[mi];
+  if (stopped(M.P)) return;  // block-uniform: the whole block returns
+  double dtc = DBL_MAX, db = 0.0;
+  if (M.P.coord == 0) update_body<0, R>(M.P, M.w, t, dtc, db);
+  else update_body<2, R>(M.P, M.w, t, dtc, db);
+  block_commit(dtc, db, M.P.scal + S_NEXT_DT, M.P.scal + S_DIVB);
+}
+template <typename R>
+__global__ void kb_wrap(const Member<R>* __restrict__ m, const unsigned long long* __restrict__ items,
+                        int axis) {
+  int mi;
+  const Pos t = item_pos(items[blockIdx.x], mi);
+  const Member<R>& M = m[mi];
+  if (stopped(M.P)) return;
+  wrap_body(M.P, axis, 0, t);
+}
+template <typename R>
+__global__ void kb_bcface(const Member<R>* __restrict__ m, const unsigned long long* __restrict__ items,
+                          int face) {
+  int mi;
+  const Pos t = item_pos(items[blockIdx.x], mi);
+  const Member<R>& M = m[mi];
+  if (stopped(M.P)) return;
+  bcface_body(M.P, face / 2, face % 2, M.bc[face], M.gbc[face], 0, t);
+}
+
 // ------------------------------------------------------ layout transposes
 
 // reference layout [f][i][j][k] (k fastest) <-> device layout
 __global__ void k_from_ref(Params P, int nf, const double* __restrict__ src, double* __restrict__ dst) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
-  int kf = blockIdx.z;
-  int k = kf % P.N[2], f = kf / P.N[2];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int kf = blockIdx.z;
+  const int k = kf % P.N[2], f = kf / P.N[2];
   if (i >= P.N[0] || j >= P.N[1] || f >= nf) return;
-  size_t r = (((size_t)f * P.N[0] + i) * P.N[1] + j) * P.N[2] + k;
+  const size_t r = (((size_t)f * P.N[0] + i) * P.N[1] + j) * P.N[2] + k;
   dst[(size_t)f * P.fs + lin(P, i, j, k)] = src[r];
 }
 
 __global__ void k_to_ref(Params P, int nf, const double* __restrict__ src, double* __restrict__ dst) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
-  int kf = blockIdx.z;
-  int k = kf % P.N[2], f = kf / P.N[2];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int kf = blockIdx.z;
+  const int k = kf % P.N[2], f = kf / P.N[2];
   if (i >= P.N[0] || j >= P.N[1] || f >= nf) return;
-  size_t r = (((size_t)f * P.N[0] + i) * P.N[1] + j) * P.N[2] + k;
+  const size_t r = (((size_t)f * P.N[0] + i) * P.N[1] + j) * P.N[2] + k;
   dst[r] = src[(size_t)f * P.fs + lin(P, i, j, k)];
 }
 
 template <typename R>
 __global__ void k_widen(Params P, int nf, const R* __restrict__ src, double* __restrict__ dst) {
-  size_t n = (size_t)nf * P.fs;
+  const size_t n = (size_t)nf * P.fs;
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
     dst[t] = (double)src[t];
 }
 
 // mags over the ghost range from face fields (for downloads)
 __global__ void k_mags(Params P, const double* __restrict__ B, double* __restrict__ out) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
-  int k = blockIdx.z * blockDim.z + threadIdx.z;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
   if (i >= P.N[0] - 1 || j >= P.N[1] - 1 || k >= P.N[2] - 1) return;
-  long long x = lin(P, i, j, k);
+  const long long x = lin(P, i, j, k);
   for (int a = 0; a < 3; a++) out[x + a * P.fs] = mags_at(P, B, a, i, j, k);
 }
 
@@ -732,64 +860,79 @@ static dim3 grid3(int a, int b, int c, dim3 blk) {
     g_launches++;                                  \
   } while (0)
 
-void launch_begin(const Params& P, cudaStream_t st) { LAUNCH(k_begin, 1, 1, st, P); }
-void launch_end(const Params& P, cudaStream_t st) { LAUNCH(k_end, 1, 1, st, P); }
-void launch_arm(const Params& P, double tstop, cudaStream_t st) { LAUNCH(k_arm, 1, 1, st, P, tstop); }
-
-void launch_dt(const Params& P, int coord, cudaStream_t st) {
-  dim3 blk(32, 4, 2);
-  dim3 g = grid3(P.n[0], P.n[1], P.n[2], blk);
-  if (coord == 0) LAUNCH(k_dt<0>, g, blk, st, P);
-  else LAUNCH(k_dt<2>, g, blk, st, P);
-}
-
 Tune::Tune() {
-  // defaults: warps along i; the sweep of D=1 / D=2 kernels runs along the
+  // defaults: warps along i; the sweeps of D=1 / D=2 kernels run along the
   // block's longer transverse side so neighbouring rows share L1 lines
   for (int t = 0; t < NTUNE; t++) blk[t] = dim3(32, 4, 2);
-  blk[K_C2C0] = blk[K_EMF0] = blk[K_FLUX0] = dim3(32, 4, 2);
   blk[K_C2C1] = blk[K_EMF1] = blk[K_FLUX1] = dim3(32, 8, 1);
   blk[K_C2C2] = blk[K_EMF2] = blk[K_FLUX2] = dim3(32, 1, 8);
 }
 
-template <typename R, int D>
-static void launch_dir(const Params& P, const Work<R>& w, cudaStream_t st, int which, dim3 blk) {
-  constexpr int p = (D + 1) % 3, q = (D + 2) % 3;
+dim3 launch_space(const Params& P, int slot) {
+  if (slot == K_AB2) return dim3(P.N[0], P.N[1], P.N[2]);
+  if (slot == K_UPDATE) return dim3(P.n[0], P.n[1], P.n[2]);
+  if (slot >= K_WRAP0 && slot <= K_WRAP2) {
+    const int a = slot - K_WRAP0;
+    return dim3(P.N[(a + 1) % 3], P.N[(a + 2) % 3], 2 * NGH);
+  }
+  if (slot >= K_BC0 && slot <= K_BC5) {
+    const int a = (slot - K_BC0) / 2;
+    return dim3(P.N[(a + 1) % 3], P.N[(a + 2) % 3], NGH);
+  }
+  const int stage = (slot - K_C2C0) / 3, D = (slot - K_C2C0) % 3;
+  const int p = (D + 1) % 3, q = (D + 2) % 3;
   int cnt[3];
-  if (which == 0) {  // first centre-to-edge sweep
+  if (stage == 0) {
     cnt[D] = P.n[D];
     cnt[p] = P.n[p] + 1;
     cnt[q] = P.n[q] + 2 * NGH;
-    LAUNCH((k_c2c<R, D>), grid3(cnt[0], cnt[1], cnt[2], blk), blk, st, P, w);
-  } else if (which == 1) {  // edge EMF
+  } else if (stage == 1) {
     cnt[D] = P.n[D];
     cnt[p] = P.n[p] + 1;
     cnt[q] = P.n[q] + 1;
-    LAUNCH((k_emf<R, D>), grid3(cnt[0], cnt[1], cnt[2], blk), blk, st, P, w);
-  } else {  // face flux
+  } else {
     cnt[0] = P.n[0];
     cnt[1] = P.n[1];
     cnt[2] = P.n[2];
     cnt[D] += 1;
-    LAUNCH((k_flux<R, D>), grid3(cnt[0], cnt[1], cnt[2], blk), blk, st, P, w);
   }
+  return dim3(cnt[0], cnt[1], cnt[2]);
+}
+
+void launch_begin(const Params& P, cudaStream_t st) { LAUNCH(k_begin, 1, 1, st, P); }
+void launch_end(const Params& P, cudaStream_t st) { LAUNCH(k_end, 1, 1, st, P); }
+void launch_arm(const Params& P, double tstop, double budget, cudaStream_t st) {
+  LAUNCH(k_arm, 1, 1, st, P, tstop, budget);
+}
+
+void launch_dt(const Params& P, int coord, cudaStream_t st) {
+  const dim3 blk(32, 4, 2);
+  const dim3 g = grid3(P.n[0], P.n[1], P.n[2], blk);
+  if (coord == 0) LAUNCH(k_dt<0>, g, blk, st, P);
+  else LAUNCH(k_dt<2>, g, blk, st, P);
 }
 
 template <typename R>
 void launch_slot(const Params& P, int coord, const Work<R>& w, int slot, dim3 blk,
                  cudaStream_t st) {
-  if (slot == K_AB2) {
-    LAUNCH(k_ab2<R>, grid3(P.N[0], P.N[1], P.N[2], blk), blk, st, P, w);
-  } else if (slot == K_UPDATE) {
-    if (coord == 0)
-      LAUNCH((k_update<0, R>), grid3(P.n[0], P.n[1], P.n[2], blk), blk, st, P, w);
-    else
-      LAUNCH((k_update<2, R>), grid3(P.n[0], P.n[1], P.n[2], blk), blk, st, P, w);
-  } else {
-    int stage = (slot - K_C2C0) / 3, d = (slot - K_C2C0) % 3;
-    if (d == 0) launch_dir<R, 0>(P, w, st, stage, blk);
-    else if (d == 1) launch_dir<R, 1>(P, w, st, stage, blk);
-    else launch_dir<R, 2>(P, w, st, stage, blk);
+  const dim3 sp = launch_space(P, slot);
+  const dim3 g = grid3(sp.x, sp.y, sp.z, blk);
+  switch (slot) {
+    case K_AB2: LAUNCH(k_ab2<R>, g, blk, st, P, w); break;
+    case K_C2C0: LAUNCH((k_c2c<R, 0>), g, blk, st, P, w); break;
+    case K_C2C1: LAUNCH((k_c2c<R, 1>), g, blk, st, P, w); break;
+    case K_C2C2: LAUNCH((k_c2c<R, 2>), g, blk, st, P, w); break;
+    case K_EMF0: LAUNCH((k_emf<R, 0>), g, blk, st, P, w); break;
+    case K_EMF1: LAUNCH((k_emf<R, 1>), g, blk, st, P, w); break;
+    case K_EMF2: LAUNCH((k_emf<R, 2>), g, blk, st, P, w); break;
+    case K_FLUX0: LAUNCH((k_flux<R, 0>), g, blk, st, P, w); break;
+    case K_FLUX1: LAUNCH((k_flux<R, 1>), g, blk, st, P, w); break;
+    case K_FLUX2: LAUNCH((k_flux<R, 2>), g, blk, st, P, w); break;
+    case K_UPDATE:
+      if (coord == 0) LAUNCH((k_update<0, R>), g, blk, st, P, w);
+      else LAUNCH((k_update<2, R>), g, blk, st, P, w);
+      break;
+    default: break;
   }
 }
 
@@ -803,10 +946,10 @@ void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t
   launch_slot<R>(P, coord, w, K_AB2, tune.blk[K_AB2], st);
   hook(G_AB2, 0);
   for (int stage = 0; stage < 3; stage++) {
-    int g = stage == 0 ? G_C2C : (stage == 1 ? G_EMF : G_FLUX);
+    const int g = stage == 0 ? G_C2C : (stage == 1 ? G_EMF : G_FLUX);
     hook(g, 1);
     for (int d = 0; d < 3; d++) {
-      int slot = K_C2C0 + 3 * stage + d;
+      const int slot = K_C2C0 + 3 * stage + d;
       launch_slot<R>(P, coord, w, slot, tune.blk[slot], st);
     }
     hook(g, 0);
@@ -823,39 +966,72 @@ template void launch_step_body<float>(const Params&, int, const Work<float>&, cu
 
 void launch_ghosts(const Params& P, const char bc[6], const char gem_bc[6], int which,
                    cudaStream_t st) {
-  dim3 blk(32, 8, 1);
+  const dim3 blk(32, 8, 1);
   bool periodic[3];
   for (int a = 0; a < 3; a++) periodic[a] = bc[2 * a] == 'p' && bc[2 * a + 1] == 'p';
   for (int a = 0; a < 3; a++) {
     if (!periodic[a]) continue;
-    int oa = (a + 1) % 3, ob = (a + 2) % 3;
-    dim3 g((P.N[oa] + blk.x - 1) / blk.x, (P.N[ob] + blk.y - 1) / blk.y, 2 * NGH);
-    // both sides in one launch: sources (active layers) and destinations
-    // (ghost layers) are disjoint for n >= NGH
-    LAUNCH(k_wrap, g, blk, st, P, a, which);
+    const dim3 sp = launch_space(P, K_WRAP0 + a);
+    LAUNCH(k_wrap, grid3(sp.x, sp.y, sp.z, blk), blk, st, P, a, which);
   }
   for (int face = 0; face < 6; face++) {
-    int a = face / 2, side = face % 2;
-    char kind = bc[face], gkind = gem_bc[face];
+    const int a = face / 2, side = face % 2;
+    const char kind = bc[face], gkind = gem_bc[face];
     if (periodic[a]) continue;
-    bool gas_work = kind != 'n';
-    bool gem_work = gkind != 'n' && gkind != 'r';
+    const bool gas_work = kind != 'n';
+    const bool gem_work = gkind != 'n' && gkind != 'r';
     if (!gas_work && !gem_work) continue;
-    int oa = (a + 1) % 3, ob = (a + 2) % 3;
-    dim3 g((P.N[oa] + blk.x - 1) / blk.x, (P.N[ob] + blk.y - 1) / blk.y, NGH);
-    LAUNCH(k_bcface, g, blk, st, P, a, side, (int)kind, (int)gkind, which);
+    const dim3 sp = launch_space(P, K_BC0 + face);
+    LAUNCH(k_bcface, grid3(sp.x, sp.y, sp.z, blk), blk, st, P, a, side, (int)kind, (int)gkind, which);
   }
 }
 
+// batched step: one launch per stage over the work lists of all members
+template <typename R>
+void launch_batch_arm(const Member<R>* m, int n, const int* steps, cudaStream_t st) {
+  LAUNCH(kb_arm<R>, (n + 127) / 128, 128, st, m, n, steps);
+}
+template void launch_batch_arm<double>(const Member<double>*, int, const int*, cudaStream_t);
+template void launch_batch_arm<float>(const Member<float>*, int, const int*, cudaStream_t);
+
+template <typename R>
+void launch_batch_step(const Member<R>* m, int n, const BatchLists& L, cudaStream_t st) {
+  const int nb = (n + 127) / 128;
+  LAUNCH(kb_begin<R>, nb, 128, st, m, n);
+#define GOP_BATCH_GO(slot, kern, ...)                                                       \
+  do {                                                                                      \
+    if (L.count[slot] > 0) LAUNCH(kern, L.count[slot], L.blk[slot], st, m, L.items[slot], ##__VA_ARGS__); \
+  } while (0)
+  GOP_BATCH_GO(K_AB2, kb_ab2<R>);
+  GOP_BATCH_GO(K_C2C0, (kb_c2c<R, 0>));
+  GOP_BATCH_GO(K_C2C1, (kb_c2c<R, 1>));
+  GOP_BATCH_GO(K_C2C2, (kb_c2c<R, 2>));
+  GOP_BATCH_GO(K_EMF0, (kb_emf<R, 0>));
+  GOP_BATCH_GO(K_EMF1, (kb_emf<R, 1>));
+  GOP_BATCH_GO(K_EMF2, (kb_emf<R, 2>));
+  GOP_BATCH_GO(K_FLUX0, (kb_flux<R, 0>));
+  GOP_BATCH_GO(K_FLUX1, (kb_flux<R, 1>));
+  GOP_BATCH_GO(K_FLUX2, (kb_flux<R, 2>));
+  GOP_BATCH_GO(K_UPDATE, kb_update<R>);
+  GOP_BATCH_GO(K_WRAP0, kb_wrap<R>, 0);
+  GOP_BATCH_GO(K_WRAP1, kb_wrap<R>, 1);
+  GOP_BATCH_GO(K_WRAP2, kb_wrap<R>, 2);
+  for (int f = 0; f < 6; f++) GOP_BATCH_GO(K_BC0 + f, kb_bcface<R>, f);
+#undef GOP_BATCH_GO
+  LAUNCH(kb_end<R>, nb, 128, st, m, n);
+}
+template void launch_batch_step<double>(const Member<double>*, int, const BatchLists&, cudaStream_t);
+template void launch_batch_step<float>(const Member<float>*, int, const BatchLists&, cudaStream_t);
+
 void launch_from_ref(const Params& P, int nf, const double* src, double* dst, cudaStream_t st) {
-  dim3 blk(32, 8, 1);
-  dim3 g((P.N[0] + 31) / 32, (P.N[1] + 7) / 8, P.N[2] * nf);
+  const dim3 blk(32, 8, 1);
+  const dim3 g((P.N[0] + 31) / 32, (P.N[1] + 7) / 8, P.N[2] * nf);
   LAUNCH(k_from_ref, g, blk, st, P, nf, src, dst);
 }
 
 void launch_to_ref(const Params& P, int nf, const double* src, double* dst, cudaStream_t st) {
-  dim3 blk(32, 8, 1);
-  dim3 g((P.N[0] + 31) / 32, (P.N[1] + 7) / 8, P.N[2] * nf);
+  const dim3 blk(32, 8, 1);
+  const dim3 g((P.N[0] + 31) / 32, (P.N[1] + 7) / 8, P.N[2] * nf);
   LAUNCH(k_to_ref, g, blk, st, P, nf, src, dst);
 }
 
@@ -867,7 +1043,7 @@ template void launch_widen<double>(const Params&, int, const double*, double*, c
 template void launch_widen<float>(const Params&, int, const float*, double*, cudaStream_t);
 
 void launch_mags(const Params& P, const double* B, double* out, cudaStream_t st) {
-  dim3 blk(32, 4, 2);
+  const dim3 blk(32, 4, 2);
   LAUNCH(k_mags, grid3(P.N[0], P.N[1], P.N[2], blk), blk, st, P, B, out);
 }
 

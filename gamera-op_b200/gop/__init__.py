@@ -256,7 +256,10 @@ class Instance:
 
 
 class Batch:
-    """Several prepared instances advanced by one graph launch per call."""
+    """Several prepared instances (any sizes, geometries, boundary kinds and
+    precisions) advanced together: every stage of a step is one launch over
+    the blocks of all members, and one captured batched step is replayed
+    max(steps) times; each member stops after its own step count."""
 
     def __init__(self, members):
         self.members = list(members)
@@ -266,6 +269,9 @@ class Batch:
         self._h = h
 
     def step(self, steps):
+        steps = list(steps)
+        if len(steps) != len(self.members):
+            raise ValueError(f"{len(steps)} step counts for {len(self.members)} members")
         arr = (C.c_int * len(self.members))(*[int(s) for s in steps])
         _check(lib().gop_batch_step(self._h, arr))
 

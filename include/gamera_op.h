@@ -211,11 +211,18 @@ int gop_problem_init(const gop_desc *desc, const gop_problem *p, double *gas, do
 /* ---- batched stepping of many independent instances ---------------- */
 typedef struct gop_batch gop_batch;
 
-/* Groups instances (all already prepared) so one call advances each by
- * its own number of steps; launches are captured in a CUDA graph. */
+/* Groups instances (all already prepared, each at most once, at most 65535)
+ * so one call advances each by its own number of steps.  Every stage of a
+ * step is one launch over the blocks of all members (a work list of
+ * (member, block) items built here), captured once in a CUDA graph; the
+ * members may differ in size, geometry, boundary kinds and precision.  The
+ * members must outlive the batch.  No counterpart in the reference, which
+ * runs one domain per process. */
 int gop_batch_create(gop_instance *const *members, int count, gop_batch **out);
 int gop_batch_destroy(gop_batch *b);
-/* steps[m] >= 0 per member; returns when all are done. */
+/* steps[m] >= 0 per member (indexed as at creation); returns when all are
+ * done.  Each member ends exactly as gop_step(member, steps[m], 1e300, ..)
+ * would leave it; GOP_ENUMERIC if any member saw a non-finite state. */
 int gop_batch_step(gop_batch *b, const int *steps);
 
 #ifdef __cplusplus

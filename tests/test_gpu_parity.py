@@ -227,6 +227,42 @@ def test_batch_results_equal_single_runs(gop):
         assert np.array_equal(d["face_b"], a["face_b"])
 
 
+def test_heterogeneous_batch_equals_members_run_alone(gop):
+    """Cartesian and spherical grids, FP64 and mixed precision, periodic and
+    outflow/reflective/fixed boundaries, uneven step budgets (0 included) in
+    one batch: every member ends bit-identical to gop_step on it alone."""
+    specs = [
+        dict(kind=gop.PROBLEM_BLAST, n=(20, 12, 8), bc="ssrrfe", b=(0.3, 0.5, 0.2), steps=6),
+        dict(kind=gop.PROBLEM_LOOP_SPH, n=(12, 10, 8), bc="eeeeee", steps=4),
+        dict(kind=gop.PROBLEM_OT, n=(24, 24, 4), bc="pppppp", domain=(0, 1, 0, 1, 0, 1 / 6),
+             precision=gop.PREC_MIXED, steps=9),
+        dict(kind=gop.PROBLEM_BLAST, n=(8, 8, 8), bc="pppppp", steps=0),
+        dict(kind=gop.PROBLEM_LOOP_CART, n=(16, 16, 16), bc="eeeeee", precision=gop.PREC_MIXED,
+             steps=5),
+    ]
+
+    def build(sp):
+        kw = {k: v for k, v in sp.items() if k not in ("kind", "n", "steps")}
+        m = gop.make(sp["kind"], sp["n"], **kw)
+        m.prepare()
+        return m
+
+    alone = []
+    for sp in specs:
+        a = build(sp)
+        a.step(sp["steps"])
+        alone.append((a.download(("gas", "face_b")), a.stats()))
+    members = [build(sp) for sp in specs]
+    b = gop.Batch(members)
+    b.step([sp["steps"] for sp in specs])
+    for (ref, st), m, sp in zip(alone, members, specs):
+        d = m.download(("gas", "face_b"))
+        assert np.array_equal(d["gas"], ref["gas"]), sp
+        assert np.array_equal(d["face_b"], ref["face_b"]), sp
+        assert m.stats()["steps"] == sp["steps"]
+        assert m.stats()["time"] == st["time"]
+
+
 def test_uneven_steps_in_one_batch(gop):
     ms = [gop.make(gop.PROBLEM_BLAST, (16, 16, 16)) for _ in range(3)]
     for m in ms:
