@@ -332,6 +332,7 @@ struct gop_instance {
   Tune tune;
   size_t bytes = 0;
   bool prepared = false;
+  bool fresh = false;  // prepared without restart and not stepped: history == state
   // per-kernel-group event timing (gop_set_profiling)
   bool prof = false;
   std::vector<cudaEvent_t> pool;
@@ -451,9 +452,11 @@ int gop_create(const gop_desc* desc, gop_instance** out) {
   size_t rsize = d.precision == GOP_PREC_MIXED ? sizeof(float) : sizeof(double);
   size_t ref = (size_t)L.N[0] * L.N[1] * L.N[2];
   cudaError_t e = cudaSuccess;
+  // stream-ordered allocations: creating and destroying instances does not
+  // wait for work of other instances or batches running on other streams
   auto alloc = [&](void** p, size_t bytes) {
     if (e == cudaSuccess) {
-      e = cudaMalloc(p, bytes);
+      e = cudaMallocAsync(p, bytes, 0);
       if (e == cudaSuccess) h->bytes += bytes;
     }
   };
@@ -462,7 +465,11 @@ int gop_create(const gop_desc* desc, gop_instance** out) {
   alloc((void**)&h->tab, T.v.size() * sizeof(double));
   alloc((void**)&h->scal, NSCAL * sizeof(double));
   alloc((void**)&h->staging, 6 * ref * sizeof(double));
-  if (e == cudaSuccess) e = cudaMallocHost((void**)&h->hscal, NSCAL * sizeof(double));
+  if (e == cudaSuccess) {
+    h->hscal = new (std::nothrow) double[NSCAL];
+    if (!h->hscal) e = cudaErrorMemoryAllocation;
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(0);
   if (e != cudaSuccess) {
     cudaGetLastError();
     gop_destroy(h);
@@ -488,7 +495,10 @@ int gop_create(const gop_desc* desc, gop_instance** out) {
     h->wd = Work<double>{w, w + 6 * L.fs, w + 9 * L.fs, w + 12 * L.fs, w + 15 * L.fs,
                          w + 21 * L.fs, w + 24 * L.fs};
   }
-  cudaError_t le = cudaDeviceSynchronize();
+  // the set-up above ran on the legacy default stream; work of batches on
+  // their own (non-blocking) streams keeps running meanwhile
+  cudaError_t le = cudaStreamSynchronize(0);
+  if (le == cudaSuccess) le = cudaGetLastError();
   if (le != cudaSuccess) {
     gop_destroy(h);
     return fail(GOP_ECUDA, "initialisation failed: %s", cudaGetErrorString(le));
@@ -499,13 +509,10 @@ int gop_create(const gop_desc* desc, gop_instance** out) {
 
 int gop_destroy(gop_instance* h) {
   if (!h) return GOP_OK;
-  if (h->st) cudaStreamSynchronize(h->st);
-  cudaFree(h->state);
-  cudaFree(h->work);
-  cudaFree(h->tab);
-  cudaFree(h->scal);
-  cudaFree(h->staging);
-  if (h->hscal) cudaFreeHost(h->hscal);
+  cudaStreamSynchronize(h->st);
+  for (void* p : {(void*)h->state, h->work, (void*)h->tab, (void*)h->scal, (void*)h->staging})
+    if (p) cudaFreeAsync(p, h->st);
+  delete[] h->hscal;
   prof_collect(h);
   for (cudaEvent_t e : h->pool) cudaEventDestroy(e);
   delete h;
@@ -581,13 +588,22 @@ int gop_prepare(gop_instance* h, int restart) {
   if (!(s[S_NEXT_DT] > 0.0) || s[S_NEXT_DT] >= DBL_MAX)
     return fail(GOP_ENUMERIC, "initial CFL dt is not positive (%g)", s[S_NEXT_DT]);
   h->prepared = true;
+  h->fresh = !restart;
   return GOP_OK;
 }
 
 }  // extern "C"
 
+// thread-block shapes the autotuners choose from (at most 256 threads)
+static const dim3 kBlockCandidates[] = {dim3(32, 4, 2), dim3(32, 8, 1), dim3(32, 1, 8),
+                                        dim3(32, 2, 4),  dim3(64, 2, 2), dim3(64, 4, 1),
+                                        dim3(64, 1, 4),  dim3(128, 2, 1), dim3(128, 1, 2),
+                                        dim3(32, 4, 1),  dim3(64, 2, 1), dim3(256, 1, 1)};
+static const int kNumBlockCandidates = sizeof(kBlockCandidates) / sizeof(kBlockCandidates[0]);
+
 static int enqueue_steps(gop_instance* h, int nsteps, double time_stop) {
   const Params& P = h->P;
+  if (nsteps > 0) h->fresh = false;
   Hook hook;
   if (h->prof) {
     hook.mark = prof_mark;
@@ -699,10 +715,8 @@ int gop_autotune(gop_instance* h, int reps, int* chosen) {
   if (!h) return fail(GOP_EINVAL, "instance is NULL");
   if (!h->prepared) return fail(GOP_ESTATE, "gop_prepare must run before gop_autotune");
   if (reps <= 0) reps = 3;
-  static const dim3 cand[] = {dim3(32, 4, 2), dim3(32, 8, 1), dim3(32, 1, 8), dim3(32, 2, 4),
-                              dim3(64, 2, 2), dim3(64, 4, 1), dim3(64, 1, 4), dim3(128, 2, 1),
-                              dim3(128, 1, 2), dim3(32, 4, 1), dim3(64, 2, 1), dim3(256, 1, 1)};
-  const int ncand = sizeof(cand) / sizeof(cand[0]);
+  const dim3* cand = kBlockCandidates;
+  const int ncand = kNumBlockCandidates;
   cudaEvent_t a, b;
   CK(cudaEventCreate(&a));
   CK(cudaEventCreate(&b));
@@ -716,7 +730,7 @@ int gop_autotune(gop_instance* h, int reps, int* chosen) {
   cur = saved_scal[S_PAR] != 0.0 ? 1 : 0;
   double* hist = nullptr;
   const size_t wbytes = (size_t)P.fs * 6 * sizeof(double), bbytes = (size_t)P.fs * 3 * sizeof(double);
-  CK(cudaMalloc((void**)&hist, wbytes + bbytes));
+  CK(cudaMallocAsync((void**)&hist, wbytes + bbytes, h->st));
   CK(cudaMemcpyAsync(hist, P.Wbuf[1 - cur], wbytes, cudaMemcpyDeviceToDevice, h->st));
   CK(cudaMemcpyAsync(hist + 6 * P.fs, P.Bbuf[1 - cur], bbytes, cudaMemcpyDeviceToDevice, h->st));
   const bool mixed = h->d.precision == GOP_PREC_MIXED;
@@ -750,7 +764,8 @@ int gop_autotune(gop_instance* h, int reps, int* chosen) {
   for (int t = 0; t < NSCAL; t++) h->hscal[t] = saved_scal[t];
   CK(cudaMemcpyAsync(h->scal, h->hscal, NSCAL * sizeof(double), cudaMemcpyHostToDevice, h->st));
   CK(cudaStreamSynchronize(h->st));
-  cudaFree(hist);
+  cudaFreeAsync(hist, h->st);
+  CK(cudaStreamSynchronize(h->st));
   CK(cudaGetLastError());
   return GOP_OK;
 }
@@ -816,9 +831,12 @@ struct gop_batch {
   std::vector<gop_instance*> m;
   std::vector<int> idx[2];  // member indices per precision (0: FP64, 1: mixed)
   BatchSide side[2];
+  Tune tune;                // block shapes of the tunable slots
   void* dev = nullptr;      // one device allocation for members, lists and steps
-  int* hsteps = nullptr;    // pinned staging of the step budgets
-  cudaStream_t st = nullptr;
+  int* hsteps = nullptr;    // host staging of the step budgets
+  int64_t nodes = 0;        // kernels in one replay of the graph
+  cudaStream_t own = nullptr;  // capture stream
+  cudaStream_t st = nullptr;   // launch stream (own, or the caller's)
   cudaGraphExec_t graph = nullptr;
 };
 
@@ -837,9 +855,120 @@ static int batch_slot_used(const gop_instance* h, int slot) {
   return gas_work || gem_work;
 }
 
-static dim3 batch_block(int slot) {
-  static const Tune defaults;
-  return slot < NTUNE ? defaults.blk[slot] : dim3(32, 8, 1);
+static dim3 batch_block(const gop_batch* b, int slot) {
+  return slot < NTUNE ? b->tune.blk[slot] : dim3(32, 8, 1);
+}
+
+// work items of one side and slot with block shape blk; false if a grid
+// needs more than 65535 blocks along an axis
+static bool batch_items(const gop_batch* b, int s, int slot, dim3 blk,
+                        std::vector<unsigned long long>& out) {
+  out.clear();
+  for (int li = 0; li < (int)b->idx[s].size(); li++) {
+    const gop_instance* h = b->m[b->idx[s][li]];
+    if (!batch_slot_used(h, slot)) continue;
+    const dim3 sp = launch_space(h->P, slot);
+    const unsigned gx = (sp.x + blk.x - 1) / blk.x, gy = (sp.y + blk.y - 1) / blk.y,
+                   gz = (sp.z + blk.z - 1) / blk.z;
+    if (gx > 0xffff || gy > 0xffff || gz > 0xffff) return false;
+    for (unsigned z = 0; z < gz; z++)
+      for (unsigned y = 0; y < gy; y++)
+        for (unsigned x = 0; x < gx; x++)
+          out.push_back(((unsigned long long)li << 48) | ((unsigned long long)x << 32) |
+                        ((unsigned long long)y << 16) | z);
+  }
+  return true;
+}
+
+static void batch_release(gop_batch* b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->dev) cudaFreeAsync(b->dev, b->own);
+  b->graph = nullptr;
+  b->dev = nullptr;
+}
+
+// (re)builds the device images of the members and work lists with the
+// batch's block shapes, and captures one batched step
+static int batch_build(gop_batch* b) {
+  batch_release(b);
+  std::vector<unsigned long long> items[2][NSLOT];
+  std::vector<Member<double>> md;
+  std::vector<Member<float>> mf;
+  for (int s = 0; s < 2; s++) {
+    for (int li = 0; li < (int)b->idx[s].size(); li++) {
+      gop_instance* h = b->m[b->idx[s][li]];
+      if (s == 0) {
+        Member<double> M{};
+        M.P = h->P;
+        M.w = h->wd;
+        for (int f = 0; f < 6; f++) M.bc[f] = h->d.bc[f], M.gbc[f] = h->d.gem_bc[f];
+        md.push_back(M);
+      } else {
+        Member<float> M{};
+        M.P = h->P;
+        M.w = h->wf;
+        for (int f = 0; f < 6; f++) M.bc[f] = h->d.bc[f], M.gbc[f] = h->d.gem_bc[f];
+        mf.push_back(M);
+      }
+    }
+    for (int slot = 0; slot < NSLOT; slot++)
+      if (!batch_items(b, s, slot, batch_block(b, slot), items[s][slot]))
+        return fail(GOP_EINVAL, "a member is too large for a batch");
+  }
+  size_t off = 0;
+  auto place = [&](size_t bytes) {
+    size_t o = (off + 255) & ~(size_t)255;
+    off = o + bytes;
+    return o;
+  };
+  size_t o_mem[2], o_items[2][NSLOT], o_steps[2];
+  o_mem[0] = place(md.size() * sizeof(Member<double>));
+  o_mem[1] = place(mf.size() * sizeof(Member<float>));
+  for (int s = 0; s < 2; s++) {
+    for (int slot = 0; slot < NSLOT; slot++) o_items[s][slot] = place(items[s][slot].size() * 8);
+    o_steps[s] = place(b->idx[s].size() * sizeof(int));
+  }
+  cudaError_t e = cudaMallocAsync(&b->dev, off, b->own);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->own);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    b->dev = nullptr;
+    return fail(GOP_ENOMEM, "batch allocation of %zu bytes failed: %s", off, cudaGetErrorString(e));
+  }
+  char* base = (char*)b->dev;
+  CK(cudaMemcpy(base + o_mem[0], md.data(), md.size() * sizeof(Member<double>), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(base + o_mem[1], mf.data(), mf.size() * sizeof(Member<float>), cudaMemcpyHostToDevice));
+  for (int s = 0; s < 2; s++) {
+    BatchSide& S = b->side[s];
+    S.n = (int)b->idx[s].size();
+    S.members = base + o_mem[s];
+    S.steps = (int*)(base + o_steps[s]);
+    for (int slot = 0; slot < NSLOT; slot++) {
+      CK(cudaMemcpy(base + o_items[s][slot], items[s][slot].data(), items[s][slot].size() * 8,
+                    cudaMemcpyHostToDevice));
+      S.L.count[slot] = (int)items[s][slot].size();
+      S.L.blk[slot] = batch_block(b, slot);
+      S.L.items[slot] = (const unsigned long long*)(base + o_items[s][slot]);
+    }
+  }
+  cudaGraph_t g = nullptr;
+  const int64_t before = launches();
+  CK(cudaStreamBeginCapture(b->own, cudaStreamCaptureModeThreadLocal));
+  if (b->side[0].n)
+    launch_batch_step<double>((const Member<double>*)b->side[0].members, b->side[0].n, b->side[0].L, b->own);
+  if (b->side[1].n)
+    launch_batch_step<float>((const Member<float>*)b->side[1].members, b->side[1].n, b->side[1].L, b->own);
+  e = cudaStreamEndCapture(b->own, &g);
+  // captured launches run at each replay, not now
+  b->nodes = launches() - before;
+  count_launches(-b->nodes);
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&b->graph, g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    b->graph = nullptr;
+    return fail(GOP_ECUDA, "batch graph capture failed: %s", cudaGetErrorString(e));
+  }
+  return GOP_OK;
 }
 
 extern "C" {
@@ -858,92 +987,21 @@ int gop_batch_create(gop_instance* const* members, int count, gop_batch** out) {
   if (!b) return fail(GOP_ENOMEM, "host allocation failed");
   b->m.assign(members, members + count);
   for (int i = 0; i < count; i++) b->idx[members[i]->d.precision == GOP_PREC_MIXED ? 1 : 0].push_back(i);
-
-  // host images: members, then per slot the work items, then step budgets
-  std::vector<unsigned long long> items[2][NSLOT];
-  std::vector<Member<double>> md;
-  std::vector<Member<float>> mf;
-  for (int s = 0; s < 2; s++) {
-    for (int li = 0; li < (int)b->idx[s].size(); li++) {
-      gop_instance* h = members[b->idx[s][li]];
-      if (s == 0) {
-        Member<double> M{};
-        M.P = h->P;
-        M.w = h->wd;
-        for (int f = 0; f < 6; f++) M.bc[f] = h->d.bc[f], M.gbc[f] = h->d.gem_bc[f];
-        md.push_back(M);
-      } else {
-        Member<float> M{};
-        M.P = h->P;
-        M.w = h->wf;
-        for (int f = 0; f < 6; f++) M.bc[f] = h->d.bc[f], M.gbc[f] = h->d.gem_bc[f];
-        mf.push_back(M);
-      }
-      for (int slot = 0; slot < NSLOT; slot++) {
-        if (!batch_slot_used(h, slot)) continue;
-        const dim3 sp = launch_space(h->P, slot), blk = batch_block(slot);
-        const unsigned gx = (sp.x + blk.x - 1) / blk.x, gy = (sp.y + blk.y - 1) / blk.y,
-                       gz = (sp.z + blk.z - 1) / blk.z;
-        if (gx > 0xffff || gy > 0xffff || gz > 0xffff) {
-          delete b;
-          return fail(GOP_EINVAL, "member %d is too large for a batch", b->idx[s][li]);
-        }
-        for (unsigned z = 0; z < gz; z++)
-          for (unsigned y = 0; y < gy; y++)
-            for (unsigned x = 0; x < gx; x++)
-              items[s][slot].push_back(((unsigned long long)li << 48) | ((unsigned long long)x << 32) |
-                                       ((unsigned long long)y << 16) | z);
-      }
-    }
+  cudaError_t e = cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking);
+  if (e == cudaSuccess) {
+    b->hsteps = new (std::nothrow) int[count];
+    if (!b->hsteps) e = cudaErrorMemoryAllocation;
   }
-  size_t off = 0;
-  auto place = [&](size_t bytes) {
-    size_t o = (off + 255) & ~(size_t)255;
-    off = o + bytes;
-    return o;
-  };
-  size_t o_mem[2], o_items[2][NSLOT], o_steps[2];
-  o_mem[0] = place(md.size() * sizeof(Member<double>));
-  o_mem[1] = place(mf.size() * sizeof(Member<float>));
-  for (int s = 0; s < 2; s++) {
-    for (int slot = 0; slot < NSLOT; slot++) o_items[s][slot] = place(items[s][slot].size() * 8);
-    o_steps[s] = place(b->idx[s].size() * sizeof(int));
-  }
-  cudaError_t e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaMalloc(&b->dev, off);
-  if (e == cudaSuccess) e = cudaMallocHost((void**)&b->hsteps, count * sizeof(int));
   if (e != cudaSuccess) {
     cudaGetLastError();
     gop_batch_destroy(b);
-    return fail(GOP_ENOMEM, "batch allocation of %zu bytes failed: %s", off, cudaGetErrorString(e));
+    return fail(GOP_ENOMEM, "batch set-up failed: %s", cudaGetErrorString(e));
   }
-  char* base = (char*)b->dev;
-  CK(cudaMemcpy(base + o_mem[0], md.data(), md.size() * sizeof(Member<double>), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(base + o_mem[1], mf.data(), mf.size() * sizeof(Member<float>), cudaMemcpyHostToDevice));
-  for (int s = 0; s < 2; s++) {
-    BatchSide& S = b->side[s];
-    S.n = (int)b->idx[s].size();
-    S.members = base + o_mem[s];
-    S.steps = (int*)(base + o_steps[s]);
-    for (int slot = 0; slot < NSLOT; slot++) {
-      CK(cudaMemcpy(base + o_items[s][slot], items[s][slot].data(), items[s][slot].size() * 8,
-                    cudaMemcpyHostToDevice));
-      S.L.count[slot] = (int)items[s][slot].size();
-      S.L.blk[slot] = batch_block(slot);
-      S.L.items[slot] = (const unsigned long long*)(base + o_items[s][slot]);
-    }
-  }
-  // one batched step of every member, captured once
-  cudaGraph_t g = nullptr;
-  CK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
-  if (b->side[0].n) launch_batch_step<double>((const Member<double>*)b->side[0].members, b->side[0].n, b->side[0].L, b->st);
-  if (b->side[1].n) launch_batch_step<float>((const Member<float>*)b->side[1].members, b->side[1].n, b->side[1].L, b->st);
-  e = cudaStreamEndCapture(b->st, &g);
-  if (e == cudaSuccess) e = cudaGraphInstantiate(&b->graph, g, 0);
-  if (g) cudaGraphDestroy(g);
-  if (e != cudaSuccess) {
+  b->st = b->own;
+  int rc = batch_build(b);
+  if (rc) {
     gop_batch_destroy(b);
-    return fail(GOP_ECUDA, "batch graph capture failed: %s", cudaGetErrorString(e));
+    return rc;
   }
   *out = b;
   return GOP_OK;
@@ -952,15 +1010,116 @@ int gop_batch_create(gop_instance* const* members, int count, gop_batch** out) {
 int gop_batch_destroy(gop_batch* b) {
   if (!b) return GOP_OK;
   if (b->st) cudaStreamSynchronize(b->st);
-  if (b->graph) cudaGraphExecDestroy(b->graph);
-  if (b->dev) cudaFree(b->dev);
-  if (b->hsteps) cudaFreeHost(b->hsteps);
-  if (b->st) cudaStreamDestroy(b->st);
+  batch_release(b);
+  delete[] b->hsteps;
+  if (b->own) cudaStreamDestroy(b->own);
   delete b;
   return GOP_OK;
 }
 
-int gop_batch_step(gop_batch* b, const int* steps) {
+int gop_batch_set_stream(gop_batch* b, void* stream) {
+  if (!b) return fail(GOP_EINVAL, "batch is NULL");
+  CK(cudaStreamSynchronize(b->st));
+  b->st = stream ? (cudaStream_t)stream : b->own;
+  return GOP_OK;
+}
+
+// Batch autotuner: for each tunable slot, times every candidate block shape
+// on the batched launch of that slot over all members and keeps the
+// fastest, then rebuilds the work lists.  The members must be freshly
+// prepared (no restart, no step yet): the history buffers then equal the
+// state, so the update launches' writes into them are undone by copying the
+// state over them again.
+int gop_batch_autotune(gop_batch* b, int reps, int* chosen) {
+  if (!b) return fail(GOP_EINVAL, "batch is NULL");
+  if (reps <= 0) reps = 3;
+  for (size_t i = 0; i < b->m.size(); i++)
+    if (!b->m[i]->fresh) return fail(GOP_ESTATE, "member %zu is not freshly prepared", i);
+  CK(cudaStreamSynchronize(b->st));
+  std::vector<std::vector<double>> saved(b->m.size());
+  for (size_t i = 0; i < b->m.size(); i++) {
+    gop_instance* h = b->m[i];
+    CK(cudaMemcpy(h->hscal, h->scal, NSCAL * sizeof(double), cudaMemcpyDeviceToHost));
+    saved[i].assign(h->hscal, h->hscal + NSCAL);
+    if (saved[i][S_PAR] != 0.0) return fail(GOP_ESTATE, "member %zu is not freshly prepared", i);
+  }
+  const int ncand = kNumBlockCandidates;
+  // largest list over candidates and slots, per side
+  size_t most = 0;
+  std::vector<unsigned long long> items;
+  for (int s = 0; s < 2; s++)
+    for (int slot = 0; slot < NTUNE; slot++)
+      for (int c = 0; c < ncand; c++) {
+        if (!batch_items(b, s, slot, kBlockCandidates[c], items)) continue;
+        most = std::max(most, items.size());
+      }
+  unsigned long long* ditems = nullptr;
+  CK(cudaMallocAsync((void**)&ditems, std::max<size_t>(most, 1) * 8, b->own));
+  CK(cudaStreamSynchronize(b->own));
+  cudaEvent_t ea, eb;
+  CK(cudaEventCreate(&ea));
+  CK(cudaEventCreate(&eb));
+  int rc = GOP_OK;
+  for (int slot = 0; slot < NTUNE && rc == GOP_OK; slot++) {
+    float best = 1e30f;
+    int best_c = -1;
+    for (int c = 0; c < ncand; c++) {
+      const dim3 blk = kBlockCandidates[c];
+      float total = 0.f;
+      bool ok = true;
+      for (int s = 0; s < 2 && ok; s++) {
+        if (!b->side[s].n) continue;
+        if (!batch_items(b, s, slot, blk, items)) {
+          ok = false;
+          break;
+        }
+        if (cudaMemcpy(ditems, items.data(), items.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess) {
+          rc = fail(GOP_ECUDA, "autotune upload failed");
+          ok = false;
+          break;
+        }
+        for (int r = 0; r <= reps; r++) {
+          if (r == 1) cudaEventRecord(ea, b->own);
+          if (s == 0)
+            launch_batch_slot<double>((const Member<double>*)b->side[0].members, slot, (int)items.size(), blk, ditems, b->own);
+          else
+            launch_batch_slot<float>((const Member<float>*)b->side[1].members, slot, (int)items.size(), blk, ditems, b->own);
+        }
+        cudaEventRecord(eb, b->own);
+        if (cudaEventSynchronize(eb) != cudaSuccess) {
+          rc = fail(GOP_ECUDA, "autotune launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+          ok = false;
+          break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ea, eb);
+        total += ms;
+      }
+      if (ok && total < best) {
+        best = total;
+        best_c = c;
+      }
+    }
+    if (best_c >= 0) b->tune.blk[slot] = kBlockCandidates[best_c];
+    if (chosen) chosen[slot] = best_c;
+  }
+  cudaEventDestroy(ea);
+  cudaEventDestroy(eb);
+  cudaFreeAsync(ditems, b->own);
+  // undo the update launches: history <- state, scalars as they were
+  for (size_t i = 0; i < b->m.size(); i++) {
+    gop_instance* h = b->m[i];
+    const Params& P = h->P;
+    CK(cudaMemcpy(P.Wbuf[1], P.Wbuf[0], (size_t)P.fs * 6 * sizeof(double), cudaMemcpyDeviceToDevice));
+    CK(cudaMemcpy(P.Bbuf[1], P.Bbuf[0], (size_t)P.fs * 3 * sizeof(double), cudaMemcpyDeviceToDevice));
+    for (int t = 0; t < NSCAL; t++) h->hscal[t] = saved[i][t];
+    CK(cudaMemcpy(h->scal, h->hscal, NSCAL * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  if (rc) return rc;
+  return batch_build(b);
+}
+
+int gop_batch_launch(gop_batch* b, const int* steps) {
   if (!b || !steps) return fail(GOP_EINVAL, "NULL argument");
   int most = 0;
   for (size_t i = 0; i < b->m.size(); i++) {
@@ -969,6 +1128,7 @@ int gop_batch_step(gop_batch* b, const int* steps) {
   }
   // members' own streams may still hold work on their state
   for (gop_instance* h : b->m) CK(cudaStreamSynchronize(h->st));
+  CK(cudaStreamSynchronize(b->st));  // the previous launch of this batch is done
   for (int s = 0; s < 2; s++) {
     BatchSide& S = b->side[s];
     if (!S.n) continue;
@@ -979,6 +1139,15 @@ int gop_batch_step(gop_batch* b, const int* steps) {
     else launch_batch_arm<float>((const Member<float>*)S.members, S.n, S.steps, b->st);
   }
   for (int n = 0; n < most; n++) CK(cudaGraphLaunch(b->graph, b->st));
+  count_launches((int64_t)most * b->nodes);
+  for (size_t i = 0; i < b->m.size(); i++)
+    if (steps[i] > 0) b->m[i]->fresh = false;
+  CK(cudaGetLastError());
+  return GOP_OK;
+}
+
+int gop_batch_wait(gop_batch* b) {
+  if (!b) return fail(GOP_EINVAL, "NULL argument");
   CK(cudaStreamSynchronize(b->st));
   CK(cudaGetLastError());
   for (gop_instance* h : b->m) {
@@ -987,6 +1156,11 @@ int gop_batch_step(gop_batch* b, const int* steps) {
     if (sc[S_FLAGS] != 0.0) return fail(GOP_ENUMERIC, "non-finite or non-positive state in a member");
   }
   return GOP_OK;
+}
+
+int gop_batch_step(gop_batch* b, const int* steps) {
+  const int rc = gop_batch_launch(b, steps);
+  return rc ? rc : gop_batch_wait(b);
 }
 
 }  // extern "C"

@@ -849,6 +849,7 @@ __global__ void k_mags(Params P, const double* __restrict__ B, double* __restric
 
 static int64_t g_launches = 0;
 int64_t launches() { return g_launches; }
+void count_launches(int64_t n) { g_launches += n; }
 
 static dim3 grid3(int a, int b, int c, dim3 blk) {
   return dim3((a + blk.x - 1) / blk.x, (b + blk.y - 1) / blk.y, (c + blk.z - 1) / blk.z);
@@ -995,29 +996,38 @@ template void launch_batch_arm<double>(const Member<double>*, int, const int*, c
 template void launch_batch_arm<float>(const Member<float>*, int, const int*, cudaStream_t);
 
 template <typename R>
+void launch_batch_slot(const Member<R>* m, int slot, int count, dim3 blk,
+                       const unsigned long long* items, cudaStream_t st) {
+  if (count <= 0) return;
+  switch (slot) {
+    case K_AB2: LAUNCH(kb_ab2<R>, count, blk, st, m, items); break;
+    case K_C2C0: LAUNCH((kb_c2c<R, 0>), count, blk, st, m, items); break;
+    case K_C2C1: LAUNCH((kb_c2c<R, 1>), count, blk, st, m, items); break;
+    case K_C2C2: LAUNCH((kb_c2c<R, 2>), count, blk, st, m, items); break;
+    case K_EMF0: LAUNCH((kb_emf<R, 0>), count, blk, st, m, items); break;
+    case K_EMF1: LAUNCH((kb_emf<R, 1>), count, blk, st, m, items); break;
+    case K_EMF2: LAUNCH((kb_emf<R, 2>), count, blk, st, m, items); break;
+    case K_FLUX0: LAUNCH((kb_flux<R, 0>), count, blk, st, m, items); break;
+    case K_FLUX1: LAUNCH((kb_flux<R, 1>), count, blk, st, m, items); break;
+    case K_FLUX2: LAUNCH((kb_flux<R, 2>), count, blk, st, m, items); break;
+    case K_UPDATE: LAUNCH(kb_update<R>, count, blk, st, m, items); break;
+    case K_WRAP0: case K_WRAP1: case K_WRAP2:
+      LAUNCH(kb_wrap<R>, count, blk, st, m, items, slot - K_WRAP0);
+      break;
+    default:
+      if (slot >= K_BC0 && slot <= K_BC5) LAUNCH(kb_bcface<R>, count, blk, st, m, items, slot - K_BC0);
+      break;
+  }
+}
+template void launch_batch_slot<double>(const Member<double>*, int, int, dim3, const unsigned long long*, cudaStream_t);
+template void launch_batch_slot<float>(const Member<float>*, int, int, dim3, const unsigned long long*, cudaStream_t);
+
+template <typename R>
 void launch_batch_step(const Member<R>* m, int n, const BatchLists& L, cudaStream_t st) {
   const int nb = (n + 127) / 128;
   LAUNCH(kb_begin<R>, nb, 128, st, m, n);
-#define GOP_BATCH_GO(slot, kern, ...)                                                       \
-  do {                                                                                      \
-    if (L.count[slot] > 0) LAUNCH(kern, L.count[slot], L.blk[slot], st, m, L.items[slot], ##__VA_ARGS__); \
-  } while (0)
-  GOP_BATCH_GO(K_AB2, kb_ab2<R>);
-  GOP_BATCH_GO(K_C2C0, (kb_c2c<R, 0>));
-  GOP_BATCH_GO(K_C2C1, (kb_c2c<R, 1>));
-  GOP_BATCH_GO(K_C2C2, (kb_c2c<R, 2>));
-  GOP_BATCH_GO(K_EMF0, (kb_emf<R, 0>));
-  GOP_BATCH_GO(K_EMF1, (kb_emf<R, 1>));
-  GOP_BATCH_GO(K_EMF2, (kb_emf<R, 2>));
-  GOP_BATCH_GO(K_FLUX0, (kb_flux<R, 0>));
-  GOP_BATCH_GO(K_FLUX1, (kb_flux<R, 1>));
-  GOP_BATCH_GO(K_FLUX2, (kb_flux<R, 2>));
-  GOP_BATCH_GO(K_UPDATE, kb_update<R>);
-  GOP_BATCH_GO(K_WRAP0, kb_wrap<R>, 0);
-  GOP_BATCH_GO(K_WRAP1, kb_wrap<R>, 1);
-  GOP_BATCH_GO(K_WRAP2, kb_wrap<R>, 2);
-  for (int f = 0; f < 6; f++) GOP_BATCH_GO(K_BC0 + f, kb_bcface<R>, f);
-#undef GOP_BATCH_GO
+  for (int slot = 0; slot < NSLOT; slot++)
+    launch_batch_slot<R>(m, slot, L.count[slot], L.blk[slot], L.items[slot], st);
   LAUNCH(kb_end<R>, nb, 128, st, m, n);
 }
 template void launch_batch_step<double>(const Member<double>*, int, const BatchLists&, cudaStream_t);

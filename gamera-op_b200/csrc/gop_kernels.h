@@ -22,6 +22,7 @@ struct Work {
 constexpr int WORK_FIELDS = 6 + 3 + 3 + 3 + 6 + 3 + 27;
 
 int64_t launches();
+void count_launches(int64_t n);  // kernels run by graph replays
 
 // kernel groups of one step, for event timing
 enum Group : int { G_BEGIN = 0, G_AB2, G_C2C, G_EMF, G_FLUX, G_UPDATE, G_GHOST, G_END, NGROUP };
@@ -88,6 +89,10 @@ template <typename R>
 void launch_batch_arm(const Member<R>* m, int n, const int* steps, cudaStream_t st);
 template <typename R>
 void launch_batch_step(const Member<R>* m, int n, const BatchLists& L, cudaStream_t st);
+// one slot's batched launch alone (for the batch autotuner)
+template <typename R>
+void launch_batch_slot(const Member<R>* m, int slot, int count, dim3 blk,
+                       const unsigned long long* items, cudaStream_t st);
 void launch_from_ref(const Params& P, int nf, const double* src, double* dst, cudaStream_t st);
 void launch_to_ref(const Params& P, int nf, const double* src, double* dst, cudaStream_t st);
 template <typename R>

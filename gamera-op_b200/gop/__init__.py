@@ -96,6 +96,10 @@ def lib():
         L.gop_batch_create.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(vp)]
         L.gop_batch_destroy.argtypes = [vp]
         L.gop_batch_step.argtypes = [vp, C.POINTER(C.c_int)]
+        L.gop_batch_launch.argtypes = [vp, C.POINTER(C.c_int)]
+        L.gop_batch_wait.argtypes = [vp]
+        L.gop_batch_set_stream.argtypes = [vp, vp]
+        L.gop_batch_autotune.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
         _lib = L
     return _lib
 
@@ -117,6 +121,15 @@ def grid_uniform(n: int, xmin: float, xmax: float) -> np.ndarray:
     x = np.zeros(n + 2 * NG + 1)
     _check(lib().gop_grid_uniform(n, xmin, xmax, _ptr(x)))
     return x
+
+
+def footprint(n, coord=COORD_CARTESIAN, precision=PREC_FP64) -> int:
+    """Device bytes gop_create would allocate for a grid (host-only)."""
+    n = tuple(int(v) for v in n)
+    xs = [np.linspace(1.0, 2.0, v + 2 * NG + 1) for v in n]
+    d = Desc(n[0], n[1], n[2], coord, _ptr(xs[0]), _ptr(xs[1]), _ptr(xs[2]), b"pppppp", b"",
+             precision, 0, 0, 0, 0, 0)
+    return int(lib().gop_footprint(C.byref(d)))
 
 
 def problem(kind: int, **over) -> Problem:
@@ -181,10 +194,17 @@ class Instance:
     def set_stream(self, stream_ptr: int):
         _check(lib().gop_set_stream(self._h, C.c_void_p(stream_ptr)))
 
-    def init_problem(self, kind: int, **over):
-        """Builds a problem's initial state on the host and uploads it."""
-        gas = np.zeros(self.shape(6))
-        fb = np.zeros(self.shape(3))
+    def init_problem(self, kind: int, out=None, **over):
+        """Builds a problem's initial state on the host (into ``out`` =
+        (gas, face_b) arrays when given, zeroed first) and returns it."""
+        if out is None:
+            gas, fb = np.zeros(self.shape(6)), np.zeros(self.shape(3))
+        else:
+            gas, fb = out
+            if gas.shape != self.shape(6) or fb.shape != self.shape(3):
+                raise ValueError("init_problem: wrong output shapes")
+            gas.fill(0.0)
+            fb.fill(0.0)
         p = problem(kind, **over)
         _check(lib().gop_problem_init(C.byref(self.desc), C.byref(p), _ptr(gas), _ptr(fb)))
         return gas, fb
@@ -274,6 +294,27 @@ class Batch:
             raise ValueError(f"{len(steps)} step counts for {len(self.members)} members")
         arr = (C.c_int * len(self.members))(*[int(s) for s in steps])
         _check(lib().gop_batch_step(self._h, arr))
+
+    def launch(self, steps):
+        """Enqueues the steps and returns at once (see wait)."""
+        steps = list(steps)
+        if len(steps) != len(self.members):
+            raise ValueError(f"{len(steps)} step counts for {len(self.members)} members")
+        arr = (C.c_int * len(self.members))(*[int(s) for s in steps])
+        _check(lib().gop_batch_launch(self._h, arr))
+
+    def wait(self):
+        _check(lib().gop_batch_wait(self._h))
+
+    def set_stream(self, stream_ptr: int):
+        _check(lib().gop_batch_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+    def autotune(self, reps=3) -> dict:
+        """Chooses block shapes for the batched launches (members must be
+        freshly prepared); returns the candidate index per launch."""
+        out = (C.c_int * len(Instance.TUNE_SLOTS))()
+        _check(lib().gop_batch_autotune(self._h, int(reps), out))
+        return dict(zip(Instance.TUNE_SLOTS, list(out)))
 
     def close(self):
         if getattr(self, "_h", None):

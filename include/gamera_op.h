@@ -224,6 +224,24 @@ int gop_batch_destroy(gop_batch *b);
  * done.  Each member ends exactly as gop_step(member, steps[m], 1e300, ..)
  * would leave it; GOP_ENUMERIC if any member saw a non-finite state. */
 int gop_batch_step(gop_batch *b, const int *steps);
+/* gop_batch_step in two halves: launch enqueues the steps on the batch's
+ * own non-blocking stream and returns; wait blocks until they are done and
+ * checks the members' flags.  Between the two the host may create, upload
+ * and prepare other instances (their set-up does not wait for the batch);
+ * it must not touch the members or destroy any instance (cudaFree waits for
+ * the whole device). */
+int gop_batch_launch(gop_batch *b, const int *steps);
+int gop_batch_wait(gop_batch *b);
+/* Launches of the batch go to `stream` (cudaStream_t as void*; NULL: the
+ * batch's own non-blocking stream). */
+int gop_batch_set_stream(gop_batch *b, void *stream);
+/* Times every candidate thread-block shape (the gop_autotune list) on the
+ * batched launch of each tunable kernel over all members, keeps the
+ * fastest and rebuilds the work lists; chosen[GOP_NTUNE] (may be NULL)
+ * receives the candidate index per kernel.  All members must be freshly
+ * prepared (gop_prepare without restart, no step since): the state and
+ * scalars are left as they were.  GOP_ESTATE otherwise. */
+int gop_batch_autotune(gop_batch *b, int reps, int *chosen);
 
 #ifdef __cplusplus
 }
