@@ -843,6 +843,8 @@ struct gop_batch {
 static int batch_slot_used(const gop_instance* h, int slot) {
   const char* bc = h->d.bc;
   const char* gbc = h->d.gem_bc;
+  if (slot == K_UPDATE) return h->d.coord == GOP_COORD_CARTESIAN;
+  if (slot == K_UPDATE_SPH) return h->d.coord != GOP_COORD_CARTESIAN;
   if (slot < NTUNE) return 1;
   if (slot <= K_WRAP2) {
     const int a = slot - K_WRAP0;
@@ -856,6 +858,7 @@ static int batch_slot_used(const gop_instance* h, int slot) {
 }
 
 static dim3 batch_block(const gop_batch* b, int slot) {
+  if (slot == K_UPDATE_SPH) return b->tune.blk[K_UPDATE];
   return slot < NTUNE ? b->tune.blk[slot] : dim3(32, 8, 1);
 }
 
@@ -1048,7 +1051,7 @@ int gop_batch_autotune(gop_batch* b, int reps, int* chosen) {
   size_t most = 0;
   std::vector<unsigned long long> items;
   for (int s = 0; s < 2; s++)
-    for (int slot = 0; slot < NTUNE; slot++)
+    for (int slot = 0; slot < NSLOT; slot++)
       for (int c = 0; c < ncand; c++) {
         if (!batch_items(b, s, slot, kBlockCandidates[c], items)) continue;
         most = std::max(most, items.size());
@@ -1067,9 +1070,11 @@ int gop_batch_autotune(gop_batch* b, int reps, int* chosen) {
       const dim3 blk = kBlockCandidates[c];
       float total = 0.f;
       bool ok = true;
-      for (int s = 0; s < 2 && ok; s++) {
+      for (int part = 0; part < 2 * (slot == K_UPDATE ? 2 : 1) && ok; part++) {
+        const int s = part % 2;
+        const int sl = part >= 2 ? K_UPDATE_SPH : slot;  // the update has two lists
         if (!b->side[s].n) continue;
-        if (!batch_items(b, s, slot, blk, items)) {
+        if (!batch_items(b, s, sl, blk, items)) {
           ok = false;
           break;
         }
@@ -1081,9 +1086,9 @@ int gop_batch_autotune(gop_batch* b, int reps, int* chosen) {
         for (int r = 0; r <= reps; r++) {
           if (r == 1) cudaEventRecord(ea, b->own);
           if (s == 0)
-            launch_batch_slot<double>((const Member<double>*)b->side[0].members, slot, (int)items.size(), blk, ditems, b->own);
+            launch_batch_slot<double>((const Member<double>*)b->side[0].members, sl, (int)items.size(), blk, ditems, b->own);
           else
-            launch_batch_slot<float>((const Member<float>*)b->side[1].members, slot, (int)items.size(), blk, ditems, b->own);
+            launch_batch_slot<float>((const Member<float>*)b->side[1].members, sl, (int)items.size(), blk, ditems, b->own);
         }
         cudaEventRecord(eb, b->own);
         if (cudaEventSynchronize(eb) != cudaSuccess) {

@@ -419,10 +419,170 @@ __device__ __forceinline__ double ct_face(const Params& P, const double* __restr
   return B[x + A * fs] - dt * (cq - cp) / Geo<COORD>::face(P, A, i, j, k);
 }
 
+// One active cell of a Cartesian grid (src/solver_solve.c:263-484 with the
+// Cartesian geometry of src/cartesian/cartesian_general.c): every face of
+// the cell has the area of its axis, every edge along axis a the length
+// dx_a, and the geometric sources vanish, so the whole cell needs dx_i,
+// dx_j, dx_k and one division.  Face fields, constrained transport, the
+// conservative update and the pressure recovery are FP64; with R = float
+// the flux divergence, the Alfven/Boris correction and the CFL estimate are
+// FP32.  Returns the cell's CFL dt and |div B| of the new state.
+template <typename R>
+__device__ __forceinline__ void update_cart(const Params& P, const Work<R>& wk, Pos t,
+                                            double& dtc, double& dbmax) {
+  const int i = NGH + t.x, j = NGH + t.y, k = NGH + t.z;
+  if (i >= NGH + P.n[0] || j >= NGH + P.n[1] || k >= NGH + P.n[2]) return;
+  const size_t fs = P.fs;
+  const double dt = P.scal[S_DT];
+  const int cb = cur_buf(P);
+  const double* __restrict__ W = P.Wbuf[cb];
+  const double* __restrict__ B = P.Bbuf[cb];
+  double* __restrict__ Wn = P.Wbuf[1 - cb];
+  double* __restrict__ Bn = P.Bbuf[1 - cb];
+  const long long x = lin(P, i, j, k), sj = P.sj, sk = P.sk;
+  const double dx[3] = {tb(P, 0, T_DX, i), tb(P, 1, T_DX, j), tb(P, 2, T_DX, k)};
+  const double A[3] = {dx[1] * dx[2], dx[0] * dx[2], dx[0] * dx[1]};
+  const double ivol = 1.0 / (dx[0] * dx[1] * dx[2]);
+  const double iA[3] = {dx[0] * ivol, dx[1] * ivol, dx[2] * ivol};  // 1/A_a
+  const double il[3] = {A[0] * ivol, A[1] * ivol, A[2] * ivol};     // 1/dx_a
+
+  // constrained transport: face A gets -dt (curl E)_A, from FP64 products
+  // of the edge EMFs and edge lengths (src/solver_solve.c:263-306)
+  const R* __restrict__ E = wk.E + x;
+  auto ed = [&](int a, long long off) { return (double)E[a * fs + off] * dx[a]; };
+  const double e0 = ed(0, 0), e1 = ed(1, 0), e2 = ed(2, 0);
+  const double e0j = ed(0, sj), e0k = ed(0, sk), e1i = ed(1, 1), e1k = ed(1, sk);
+  const double e2i = ed(2, 1), e2j = ed(2, sj);
+  double bl[3], bu[3], mo[3];
+  bl[0] = B[x] - dt * ((e2j - e2) - (e1k - e1)) * iA[0];
+  bl[1] = B[x + fs] - dt * ((e0k - e0) - (e2i - e2)) * iA[1];
+  bl[2] = B[x + 2 * fs] - dt * ((e1i - e1) - (e0j - e0)) * iA[2];
+  {
+    const double e1ik = ed(1, 1 + sk), e2ij = ed(2, 1 + sj), e0jk = ed(0, sj + sk);
+    bu[0] = B[x + 1] - dt * ((e2ij - e2i) - (e1ik - e1i)) * iA[0];
+    bu[1] = B[x + sj + fs] - dt * ((e0jk - e0j) - (e2ij - e2j)) * iA[1];
+    bu[2] = B[x + sk + 2 * fs] - dt * ((e1ik - e1k) - (e0jk - e0k)) * iA[2];
+  }
+  // mags^n for the time-centred field
+  mo[0] = B[x] * tb(P, 0, T_MA, i) + B[x + 1] * tb(P, 0, T_MB, i);
+  mo[1] = B[x + fs] * tb(P, 1, T_MA, j) + B[x + sj + fs] * tb(P, 1, T_MB, j);
+  mo[2] = B[x + 2 * fs] * tb(P, 2, T_MA, k) + B[x + sk + 2 * fs] * tb(P, 2, T_MB, k);
+  Bn[x] = bl[0];
+  Bn[x + fs] = bl[1];
+  Bn[x + 2 * fs] = bl[2];
+  if (i == NGH + P.n[0] - 1) Bn[x + 1] = bu[0];
+  if (j == NGH + P.n[1] - 1) Bn[x + sj + fs] = bu[1];
+  if (k == NGH + P.n[2] - 1) Bn[x + sk + 2 * fs] = bu[2];
+  {
+    const double dvb = (bu[0] * A[0] - bl[0] * A[0]) * ivol + (bu[1] * A[1] - bl[1] * A[1]) * ivol +
+                       (bu[2] * A[2] - bl[2] * A[2]) * ivol;
+    dbmax = fabs(dvb);
+  }
+  double mn[3], mt[3];
+  mn[0] = bl[0] * tb(P, 0, T_MA, i) + bu[0] * tb(P, 0, T_MB, i);
+  mn[1] = bl[1] * tb(P, 1, T_MA, j) + bu[1] * tb(P, 1, T_MB, j);
+  mn[2] = bl[2] * tb(P, 2, T_MA, k) + bu[2] * tb(P, 2, T_MB, k);
+#pragma unroll
+  for (int a = 0; a < 3; a++) mt[a] = 0.5 * (mn[a] + mo[a]);
+
+  // flux divergence: 6 hydro and 3 stress components (R arithmetic when
+  // R = float; the reference's F_u A - F_l A over the volume otherwise)
+  R du[6], dm[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const long long s = d == 0 ? 1LL : (d == 1 ? sj : sk);
+    const R* __restrict__ Fd = wk.F + (size_t)(9 * d) * fs + x;
+#pragma unroll
+    for (int m = 0; m < 9; m++) {
+      R v;
+      if constexpr (sizeof(R) == 4) {
+        v = (Fd[s + m * fs] - Fd[m * fs]) * (R)il[d];
+      } else {
+        v = (Fd[s + m * fs] * A[d] - Fd[m * fs] * A[d]) * ivol;
+      }
+      if (m < 6) du[m] = d == 0 ? v : du[m] + v;
+      else dm[m - 6] = d == 0 ? v : dm[m - 6] + v;
+    }
+  }
+
+  // U^n from W^n, conservative update, cons->prim in FP64
+  // (src/solver_func.c:356-382, src/solver_solve.c:326-377)
+  const double gm1 = P.gm1;
+  const double r0 = W[x], u0 = W[x + fs], v0 = W[x + 2 * fs], w0 = W[x + 3 * fs],
+               p0 = W[x + 4 * fs], ps0 = W[x + 5 * fs];
+  const double U0[3] = {r0 * u0, r0 * v0, r0 * w0};
+  const double E0 = 0.5 * r0 * (u0 * u0 + v0 * v0 + w0 * w0) + p0 * P.inv_gm1;
+  const double S0 = (ps0 == 0.0 && r0 > 0.0) ? ps0 : ps0 / pow(r0, gm1);
+  const double Ur = r0 - dt * (double)du[0];
+  double Um[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) Um[a] = U0[a] - dt * (double)du[1 + a];
+  const double Ue = E0 - dt * (double)du[4];
+  const double Us = S0 - dt * (double)du[5];
+  double rho = Ur;
+  const double irho = 1.0 / Ur;
+  double vv[3] = {Um[0] * irho, Um[1] * irho, Um[2] * irho};
+  double p = (Ue - 0.5 * (vv[0] * vv[0] + vv[1] * vv[1] + vv[2] * vv[2]) * rho) * gm1;
+  const double pS = (Us == 0.0 && Ur > 0.0) ? Us : Us * pow(Ur, gm1);
+  // positivity floors (src/solver_func.c:2117-2135)
+  if (rho < P.rho_floor) {
+    rho = P.rho_floor;
+    p = P.p_floor;
+  }
+  if (p < P.p_floor) p = P.p_floor;
+
+  // Alfven/Boris correction of the momentum (src/solver_solve.c:385-484)
+  {
+    const R bsq = (R)(mt[0] * mt[0] + mt[1] * mt[1] + mt[2] * mt[2]);
+    const R alf = bsq / ((R)rho * (R)P.ca2);
+    const R perp = R(1) / (R(1) + alf);
+    const R rdt = (R)dt;
+    const R drho = -rdt * du[0];
+    const R dva = alf * drho;
+    R tv[3], wv[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      wv[a] = (R)W[x + (1 + a) * fs];
+      tv[a] = alf * (-rdt * du[1 + a] - drho * wv[a]);
+    }
+    R bdv = (R)mt[0] * tv[0] + (R)mt[1] * tv[1] + (R)mt[2] * tv[2];
+    bdv = bdv / (bsq + R(1e-10));
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const R inc = perp * ((-rdt * du[1 + a]) + (-rdt * dm[a]) + dva * wv[a] + (R)mt[a] * bdv);
+      vv[a] = (U0[a] + (double)inc) * irho;
+    }
+  }
+  Wn[x] = rho;
+  Wn[x + fs] = vv[0];
+  Wn[x + 2 * fs] = vv[1];
+  Wn[x + 3 * fs] = vv[2];
+  Wn[x + 4 * fs] = p;
+  Wn[x + 5 * fs] = pS;
+
+  // CFL dt of the new state with magtot = mags^{n+1} (src/solver_func.c:255-298)
+  {
+    const R r = (R)rho, u = (R)vv[0], v = (R)vv[1], w = (R)vv[2];
+    const R bsq = (R)(mn[0] * mn[0] + mn[1] * mn[1] + mn[2] * mn[2]);
+    const R va = sqrt(bsq / r);
+    const R vae = va * (R)P.ca / sqrt(va * va + (R)P.ca2);
+    const R vf = sqrt(u * u + v * v + w * w);
+    const R vs = sqrt((R)P.gamma * (R)p / r);
+    const R vc = vf + sqrt(vs * vs + vae * vae);
+    dtc = (double)((R)P.cfl / (vc * (R)il[0] + vc * (R)il[1] + vc * (R)il[2]));
+  }
+  if (!(dtc > 0.0) || !isfinite(p) || !isfinite(rho) || !isfinite(vv[0] + vv[1] + vv[2]))
+    P.scal[S_FLAGS] = 1.0;
+}
+
 // one active cell: returns its CFL dt and |div B| of the new state
 template <int COORD, typename R>
 __device__ __forceinline__ void update_body(const Params& P, const Work<R>& wk, Pos t,
                                             double& dtc, double& dbmax) {
+  if constexpr (COORD == 0) {
+    update_cart<R>(P, wk, t, dtc, dbmax);
+    return;
+  }
   const int i = NGH + t.x, j = NGH + t.y, k = NGH + t.z;
   if (i >= NGH + P.n[0] || j >= NGH + P.n[1] || k >= NGH + P.n[2]) return;
   const size_t fs = P.fs;
@@ -671,6 +831,45 @@ __device__ __forceinline__ void bcface_body(const Params& P, int axis, int side,
 
 // ------------------------------------------------- single-instance kernels
 
+// Resident 256-thread blocks per SM each kernel is compiled for (caps its
+// registers at 65536 / (256 * n)), per stage and arithmetic type; the
+// defaults are the fastest of 1..4 timed on B200 (blast 256^3).
+#ifndef GOP_MINB_AB2_F64
+#define GOP_MINB_AB2_F64 1
+#endif
+#ifndef GOP_MINB_AB2_F32
+#define GOP_MINB_AB2_F32 1
+#endif
+#ifndef GOP_MINB_C2C_F64
+#define GOP_MINB_C2C_F64 3
+#endif
+#ifndef GOP_MINB_C2C_F32
+#define GOP_MINB_C2C_F32 4
+#endif
+#ifndef GOP_MINB_EMF_F64
+#define GOP_MINB_EMF_F64 2
+#endif
+#ifndef GOP_MINB_EMF_F32
+#define GOP_MINB_EMF_F32 4
+#endif
+#ifndef GOP_MINB_FLUX_F64
+#define GOP_MINB_FLUX_F64 2
+#endif
+#ifndef GOP_MINB_FLUX_F32
+#define GOP_MINB_FLUX_F32 4
+#endif
+#ifndef GOP_MINB_UPDATE_F64
+#define GOP_MINB_UPDATE_F64 3
+#endif
+#ifndef GOP_MINB_UPDATE_F32
+#define GOP_MINB_UPDATE_F32 4
+#endif
+#ifndef GOP_MINB_UPDATE_SPH
+#define GOP_MINB_UPDATE_SPH 2
+#endif
+#define GOP_MINB(STAGE, R) (sizeof(R) == 8 ? GOP_MINB_##STAGE##_F64 : GOP_MINB_##STAGE##_F32)
+#define GOP_UPD_MINB(COORD, R) ((COORD) == 0 ? GOP_MINB(UPDATE, R) : GOP_MINB_UPDATE_SPH)
+
 __global__ void k_begin(Params P) { begin_body(P); }
 __global__ void k_end(Params P) { end_body(P); }
 __global__ void k_arm(Params P, double tstop, double budget) { arm_body(P, tstop, budget); }
@@ -683,27 +882,27 @@ __global__ void k_dt(Params P) {
 }
 
 template <typename R>
-__global__ void __launch_bounds__(256) k_ab2(Params P, Work<R> w) {
+__global__ void __launch_bounds__(256, GOP_MINB(AB2, R)) k_ab2(Params P, Work<R> w) {
   if (stopped(P)) return;
   ab2_body<R>(P, w, grid_pos());
 }
 template <typename R, int D>
-__global__ void __launch_bounds__(256) k_c2c(Params P, Work<R> w) {
+__global__ void __launch_bounds__(256, GOP_MINB(C2C, R)) k_c2c(Params P, Work<R> w) {
   if (stopped(P)) return;
   c2c_body<R, D>(P, w, grid_pos());
 }
 template <typename R, int D>
-__global__ void __launch_bounds__(256) k_emf(Params P, Work<R> w) {
+__global__ void __launch_bounds__(256, GOP_MINB(EMF, R)) k_emf(Params P, Work<R> w) {
   if (stopped(P)) return;
   emf_body<R, D>(P, w, grid_pos());
 }
 template <typename R, int D>
-__global__ void __launch_bounds__(256, 2) k_flux(Params P, Work<R> w) {
+__global__ void __launch_bounds__(256, GOP_MINB(FLUX, R)) k_flux(Params P, Work<R> w) {
   if (stopped(P)) return;
   flux_body<R, D>(P, w, grid_pos());
 }
 template <int COORD, typename R>
-__global__ void __launch_bounds__(256) k_update(Params P, Work<R> w) {
+__global__ void __launch_bounds__(256, GOP_UPD_MINB(COORD, R)) k_update(Params P, Work<R> w) {
   if (stopped(P)) return;
   double dtc = DBL_MAX, db = 0.0;
   update_body<COORD, R>(P, w, grid_pos(), dtc, db);
@@ -739,7 +938,7 @@ __global__ void kb_arm(const Member<R>* __restrict__ m, int n, const int* __rest
 }
 
 template <typename R>
-__global__ void __launch_bounds__(256) kb_ab2(const Member<R>* __restrict__ m,
+__global__ void __launch_bounds__(256, GOP_MINB(AB2, R)) kb_ab2(const Member<R>* __restrict__ m,
                                               const unsigned long long* __restrict__ items) {
   int mi;
   const Pos t = item_pos(items[blockIdx.x], mi);
@@ -748,7 +947,7 @@ __global__ void __launch_bounds__(256) kb_ab2(const Member<R>* __restrict__ m,
   ab2_body<R>(M.P, M.w, t);
 }
 template <typename R, int D>
-__global__ void __launch_bounds__(256) kb_c2c(const Member<R>* __restrict__ m,
+__global__ void __launch_bounds__(256, GOP_MINB(C2C, R)) kb_c2c(const Member<R>* __restrict__ m,
                                               const unsigned long long* __restrict__ items) {
   int mi;
   const Pos t = item_pos(items[blockIdx.x], mi);
@@ -757,7 +956,7 @@ __global__ void __launch_bounds__(256) kb_c2c(const Member<R>* __restrict__ m,
   c2c_body<R, D>(M.P, M.w, t);
 }
 template <typename R, int D>
-__global__ void __launch_bounds__(256) kb_emf(const Member<R>* __restrict__ m,
+__global__ void __launch_bounds__(256, GOP_MINB(EMF, R)) kb_emf(const Member<R>* __restrict__ m,
                                               const unsigned long long* __restrict__ items) {
   int mi;
   const Pos t = item_pos(items[blockIdx.x], mi);
@@ -766,7 +965,7 @@ __global__ void __launch_bounds__(256) kb_emf(const Member<R>* __restrict__ m,
   emf_body<R, D>(M.P, M.w, t);
 }
 template <typename R, int D>
-__global__ void __launch_bounds__(256, 2) kb_flux(const Member<R>* __restrict__ m,
+__global__ void __launch_bounds__(256, GOP_MINB(FLUX, R)) kb_flux(const Member<R>* __restrict__ m,
                                                   const unsigned long long* __restrict__ items) {
   int mi;
   const Pos t = item_pos(items[blockIdx.x], mi);
@@ -774,16 +973,17 @@ __global__ void __launch_bounds__(256, 2) kb_flux(const Member<R>* __restrict__ 
   if (stopped(M.P)) return;
   flux_body<R, D>(M.P, M.w, t);
 }
-template <typename R>
-__global__ void __launch_bounds__(256) kb_update(const Member<R>* __restrict__ m,
-                                                 const unsigned long long* __restrict__ items) {
+// Cartesian and spherical members have separate work lists (K_UPDATE,
+// K_UPDATE_SPH) so each kernel is compiled for one geometry
+template <int COORD, typename R>
+__global__ void __launch_bounds__(256, GOP_UPD_MINB(COORD, R)) kb_update(const Member<R>* __restrict__ m,
+                                                    const unsigned long long* __restrict__ items) {
   int mi;
   const Pos t = item_pos(items[blockIdx.x], mi);
   const Member<R>& M = m[mi];
   if (stopped(M.P)) return;  // block-uniform: the whole block returns
   double dtc = DBL_MAX, db = 0.0;
-  if (M.P.coord == 0) update_body<0, R>(M.P, M.w, t, dtc, db);
-  else update_body<2, R>(M.P, M.w, t, dtc, db);
+  update_body<COORD, R>(M.P, M.w, t, dtc, db);
   block_commit(dtc, db, M.P.scal + S_NEXT_DT, M.P.scal + S_DIVB);
 }
 template <typename R>
@@ -871,7 +1071,7 @@ Tune::Tune() {
 
 dim3 launch_space(const Params& P, int slot) {
   if (slot == K_AB2) return dim3(P.N[0], P.N[1], P.N[2]);
-  if (slot == K_UPDATE) return dim3(P.n[0], P.n[1], P.n[2]);
+  if (slot == K_UPDATE || slot == K_UPDATE_SPH) return dim3(P.n[0], P.n[1], P.n[2]);
   if (slot >= K_WRAP0 && slot <= K_WRAP2) {
     const int a = slot - K_WRAP0;
     return dim3(P.N[(a + 1) % 3], P.N[(a + 2) % 3], 2 * NGH);
@@ -1010,7 +1210,8 @@ void launch_batch_slot(const Member<R>* m, int slot, int count, dim3 blk,
     case K_FLUX0: LAUNCH((kb_flux<R, 0>), count, blk, st, m, items); break;
     case K_FLUX1: LAUNCH((kb_flux<R, 1>), count, blk, st, m, items); break;
     case K_FLUX2: LAUNCH((kb_flux<R, 2>), count, blk, st, m, items); break;
-    case K_UPDATE: LAUNCH(kb_update<R>, count, blk, st, m, items); break;
+    case K_UPDATE: LAUNCH((kb_update<0, R>), count, blk, st, m, items); break;
+    case K_UPDATE_SPH: LAUNCH((kb_update<2, R>), count, blk, st, m, items); break;
     case K_WRAP0: case K_WRAP1: case K_WRAP2:
       LAUNCH(kb_wrap<R>, count, blk, st, m, items, slot - K_WRAP0);
       break;
@@ -1026,7 +1227,12 @@ template <typename R>
 void launch_batch_step(const Member<R>* m, int n, const BatchLists& L, cudaStream_t st) {
   const int nb = (n + 127) / 128;
   LAUNCH(kb_begin<R>, nb, 128, st, m, n);
-  for (int slot = 0; slot < NSLOT; slot++)
+  // the stages in step order; the ghost fill after both updates
+  for (int slot = 0; slot <= K_UPDATE; slot++)
+    launch_batch_slot<R>(m, slot, L.count[slot], L.blk[slot], L.items[slot], st);
+  launch_batch_slot<R>(m, K_UPDATE_SPH, L.count[K_UPDATE_SPH], L.blk[K_UPDATE_SPH],
+                       L.items[K_UPDATE_SPH], st);
+  for (int slot = K_WRAP0; slot <= K_BC5; slot++)
     launch_batch_slot<R>(m, slot, L.count[slot], L.blk[slot], L.items[slot], st);
   LAUNCH(kb_end<R>, nb, 128, st, m, n);
 }

@@ -28,12 +28,14 @@ void count_launches(int64_t n);  // kernels run by graph replays
 enum Group : int { G_BEGIN = 0, G_AB2, G_C2C, G_EMF, G_FLUX, G_UPDATE, G_GHOST, G_END, NGROUP };
 
 // launch shapes of the tunable kernels: AB2, C2C x3, EMF x3, FLUX x3, UPDATE;
-// then the ghost launches (periodic wrap per axis, boundary fill per face),
-// which have their own slots in the batched work lists only
+// then the slots of the batched work lists only: the ghost launches
+// (periodic wrap per axis, boundary fill per face) and the update of
+// spherical members (K_UPDATE then holds the Cartesian ones; both use the
+// UPDATE block shape)
 enum TuneSlot : int { K_AB2 = 0, K_C2C0, K_C2C1, K_C2C2, K_EMF0, K_EMF1, K_EMF2,
                       K_FLUX0, K_FLUX1, K_FLUX2, K_UPDATE, NTUNE,
                       K_WRAP0 = NTUNE, K_WRAP1, K_WRAP2, K_BC0, K_BC1, K_BC2, K_BC3, K_BC4,
-                      K_BC5, NSLOT };
+                      K_BC5, K_UPDATE_SPH, NSLOT };
 struct Tune {
   dim3 blk[NTUNE];
   Tune();
