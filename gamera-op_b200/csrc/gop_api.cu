@@ -324,6 +324,7 @@ struct gop_instance {
   double* state = nullptr;   // 2 x (6 + 3) fields
   void* work = nullptr;      // WORK_FIELDS x R
   double* tab = nullptr;
+  float* tabf = nullptr;     // FP32 copy of the tables (mixed path)
   double* scal = nullptr;
   double* staging = nullptr; // reference-layout scratch, 6 x NI*NJ*NK
   double* hscal = nullptr;   // pinned host copy of the scalars
@@ -394,8 +395,10 @@ size_t gop_footprint(const gop_desc* d) {
   size_t rsize = d->precision == GOP_PREC_MIXED ? sizeof(float) : sizeof(double);
   size_t ref = (size_t)L.N[0] * L.N[1] * L.N[2];
   size_t tmax = std::max(L.N[0], std::max(L.N[1], L.N[2])) + 1;
-  return (size_t)L.fs * (18 * sizeof(double) + WORK_FIELDS * rsize) + 6 * ref * sizeof(double) +
-         3 * NTAB * tmax * sizeof(double) + NSCAL * sizeof(double);
+  const bool mixed = d->precision == GOP_PREC_MIXED;
+  return (size_t)L.fs * (18 * sizeof(double) + work_fields(mixed) * rsize) +
+         6 * ref * sizeof(double) + 3 * NTAB * tmax * (sizeof(double) + (mixed ? sizeof(float) : 0)) +
+         NSCAL * sizeof(double);
 }
 
 int gop_create(const gop_desc* desc, gop_instance** out) {
@@ -460,9 +463,12 @@ int gop_create(const gop_desc* desc, gop_instance** out) {
       if (e == cudaSuccess) h->bytes += bytes;
     }
   };
+  const bool mixed = d.precision == GOP_PREC_MIXED;
+  const int nwork = work_fields(mixed);
   alloc((void**)&h->state, (size_t)L.fs * 18 * sizeof(double));
-  alloc(&h->work, (size_t)L.fs * WORK_FIELDS * rsize);
+  alloc(&h->work, (size_t)L.fs * nwork * rsize);
   alloc((void**)&h->tab, T.v.size() * sizeof(double));
+  if (mixed) alloc((void**)&h->tabf, T.v.size() * sizeof(float));
   alloc((void**)&h->scal, NSCAL * sizeof(double));
   alloc((void**)&h->staging, 6 * ref * sizeof(double));
   if (e == cudaSuccess) {
@@ -477,8 +483,12 @@ int gop_create(const gop_desc* desc, gop_instance** out) {
                 cudaGetErrorString(e));
   }
   cudaMemset(h->state, 0, (size_t)L.fs * 18 * sizeof(double));
-  cudaMemset(h->work, 0, (size_t)L.fs * WORK_FIELDS * rsize);
+  cudaMemset(h->work, 0, (size_t)L.fs * nwork * rsize);
   cudaMemcpy(h->tab, T.v.data(), T.v.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (mixed) {
+    std::vector<float> tf(T.v.begin(), T.v.end());
+    cudaMemcpy(h->tabf, tf.data(), tf.size() * sizeof(float), cudaMemcpyHostToDevice);
+  }
   cudaMemset(h->scal, 0, NSCAL * sizeof(double));
   P.tab = h->tab;
   P.scal = h->scal;
@@ -489,11 +499,11 @@ int gop_create(const gop_desc* desc, gop_instance** out) {
   if (d.precision == GOP_PREC_MIXED) {
     float* w = (float*)h->work;
     h->wf = Work<float>{w, w + 6 * L.fs, w + 9 * L.fs, w + 12 * L.fs, w + 15 * L.fs,
-                        w + 21 * L.fs, w + 24 * L.fs};
+                        w + 21 * L.fs, w + 24 * L.fs, w + 51 * L.fs, w + 57 * L.fs, h->tabf};
   } else {
     double* w = (double*)h->work;
     h->wd = Work<double>{w, w + 6 * L.fs, w + 9 * L.fs, w + 12 * L.fs, w + 15 * L.fs,
-                         w + 21 * L.fs, w + 24 * L.fs};
+                         w + 21 * L.fs, w + 24 * L.fs, nullptr, nullptr, h->tab};
   }
   // the set-up above ran on the legacy default stream; work of batches on
   // their own (non-blocking) streams keeps running meanwhile
@@ -510,7 +520,8 @@ int gop_create(const gop_desc* desc, gop_instance** out) {
 int gop_destroy(gop_instance* h) {
   if (!h) return GOP_OK;
   cudaStreamSynchronize(h->st);
-  for (void* p : {(void*)h->state, h->work, (void*)h->tab, (void*)h->scal, (void*)h->staging})
+  for (void* p : {(void*)h->state, h->work, (void*)h->tab, (void*)h->tabf, (void*)h->scal,
+                  (void*)h->staging})
     if (p) cudaFreeAsync(p, h->st);
   delete[] h->hscal;
   prof_collect(h);

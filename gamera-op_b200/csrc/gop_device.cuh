@@ -162,17 +162,20 @@ struct FaceWeights {
   R wl[7], wr[7], cl1, cl2, cr1, cr2;
 };
 
+// tab: the per-axis tables in the stage type R (layout of Params::tab)
 template <typename R>
-__device__ __forceinline__ void load_weights(const Params& P, int axis, int f, FaceWeights<R>& W) {
+__device__ __forceinline__ void load_weights(const R* __restrict__ tab, int tmax, int axis, int f,
+                                             FaceWeights<R>& W) {
+  const R* t0 = tab + (size_t)axis * NTAB * tmax + f;
 #pragma unroll
   for (int t = 0; t < 7; t++) {
-    W.wl[t] = (R)tb(P, axis, T_WL0 + t, f);
-    W.wr[t] = (R)tb(P, axis, T_WR0 + t, f);
+    W.wl[t] = __ldg(t0 + (size_t)(T_WL0 + t) * tmax);
+    W.wr[t] = __ldg(t0 + (size_t)(T_WR0 + t) * tmax);
   }
-  W.cl1 = (R)tb(P, axis, T_CL1, f);
-  W.cl2 = (R)tb(P, axis, T_CL2, f);
-  W.cr1 = (R)tb(P, axis, T_CR1, f);
-  W.cr2 = (R)tb(P, axis, T_CR2, f);
+  W.cl1 = __ldg(t0 + (size_t)T_CL1 * tmax);
+  W.cl2 = __ldg(t0 + (size_t)T_CL2 * tmax);
+  W.cr1 = __ldg(t0 + (size_t)T_CR1 * tmax);
+  W.cr2 = __ldg(t0 + (size_t)T_CR2 * tmax);
 }
 
 template <typename R>

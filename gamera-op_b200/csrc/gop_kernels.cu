@@ -121,6 +121,20 @@ __device__ __forceinline__ void line8(const T* __restrict__ a, long long s, R v[
 __device__ __forceinline__ double rsq(double x) { return rsqrt(x); }
 __device__ __forceinline__ float rsq(float x) { return rsqrtf(x); }
 
+// The step-start state the PDM limiters compare against, in the stage type:
+// the FP64 state itself on the plain path, its FP32 copy (written by the
+// AB2 stage) on the mixed path.
+template <typename R>
+__device__ __forceinline__ const R* lim_w(const Params& P, const Work<R>& wk) {
+  if constexpr (sizeof(R) == 8) return reinterpret_cast<const R*>(P.Wbuf[cur_buf(P)]);
+  else return wk.Wl;
+}
+template <typename R>
+__device__ __forceinline__ const R* lim_b(const Params& P, const Work<R>& wk) {
+  if constexpr (sizeof(R) == 8) return reinterpret_cast<const R*>(P.Bbuf[cur_buf(P)]);
+  else return wk.Bl;
+}
+
 // thread coordinates in a launch space
 struct Pos {
   int x, y, z;
@@ -195,6 +209,7 @@ __device__ __forceinline__ void ab2_body(const Params& P, const Work<R>& w, Pos 
     for (int m = 0; m < 6; m++) {
       const double v = W[x + m * fs], vo = Wo[x + m * fs];
       w.Wh[x + m * fs] = (R)(v + c * (v - vo));
+      if constexpr (sizeof(R) == 4) w.Wl[x + m * fs] = (R)v;
     }
 #pragma unroll
     for (int a = 0; a < 3; a++) {
@@ -209,6 +224,7 @@ __device__ __forceinline__ void ab2_body(const Params& P, const Work<R>& w, Pos 
     if (ok) {
       const double b = B[x + a * fs], bo = Bo[x + a * fs];
       w.Bh[x + a * fs] = (R)(b + c * (b - bo));
+      if constexpr (sizeof(R) == 4) w.Bl[x + a * fs] = (R)b;
     }
   }
 }
@@ -232,9 +248,9 @@ __device__ __forceinline__ void c2c_body(const Params& P, const Work<R>& wk, Pos
   const int f = p == 0 ? i : (p == 1 ? j : k);
   const long long x = lin(P, i, j, k), s = sd<p>(P);
   const size_t fs = P.fs;
-  const double* __restrict__ W = P.Wbuf[cur_buf(P)] + x;
+  const R* __restrict__ W = lim_w<R>(P, wk) + x;
   FaceWeights<R> Wt;
-  load_weights<R>(P, p, f, Wt);
+  load_weights<R>(wk.tab, P.tmax, p, f, Wt);
   const R a1 = (R)P.pdm_a1, a2 = (R)P.pdm_a2;
 #pragma unroll
   for (int cc = 0; cc < 2; cc++) {
@@ -242,7 +258,7 @@ __device__ __forceinline__ void c2c_body(const Params& P, const Work<R>& wk, Pos
     R v[8], lim[4], L, Rr;
     line8<R, R>(wk.Wh + (size_t)(V1 + comp) * fs + x, s, v);
 #pragma unroll
-    for (int u = 0; u < 4; u++) lim[u] = (R)W[(V1 + comp) * fs + (u - 2) * s];
+    for (int u = 0; u < 4; u++) lim[u] = W[(V1 + comp) * fs + (u - 2) * s];
     recon_lr<R>(v, lim, Wt, a1, a2, L, Rr);
     wk.V[x + (size_t)(2 * D + cc) * fs] = R(0.5) * (L + Rr);
   }
@@ -263,12 +279,12 @@ __device__ __forceinline__ void emf_body(const Params& P, const Work<R>& wk, Pos
   const int pos[3] = {i, j, k};
   const long long x = lin(P, i, j, k), sp = sd<p>(P), sq = sd<q>(P);
   const size_t fs = P.fs;
-  const double* __restrict__ B = P.Bbuf[cur_buf(P)] + x;
+  const R* __restrict__ B = lim_b<R>(P, wk) + x;
   const R a1 = (R)P.pdm_a1, a2 = (R)P.pdm_a2;
   R vav[2], bpl, bpr, bql, bqr;
   {
     FaceWeights<R> Wt;
-    load_weights<R>(P, q, pos[q], Wt);
+    load_weights<R>(wk.tab, P.tmax, q, pos[q], Wt);
 #pragma unroll
     for (int cc = 0; cc < 2; cc++) {
       R v[8], lim[4], L, Rr;
@@ -282,17 +298,17 @@ __device__ __forceinline__ void emf_body(const Params& P, const Work<R>& wk, Pos
     R v[8], lim[4];
     line8<R, R>(wk.Bh + (size_t)p * fs + x, sq, v);
 #pragma unroll
-    for (int u = 0; u < 4; u++) lim[u] = (R)B[p * fs + (u - 2) * sq];
+    for (int u = 0; u < 4; u++) lim[u] = B[p * fs + (u - 2) * sq];
     recon_lr<R>(v, lim, Wt, a1, a2, bpl, bpr);
   }
   {
     // B_q along p
     FaceWeights<R> Wt;
-    load_weights<R>(P, p, pos[p], Wt);
+    load_weights<R>(wk.tab, P.tmax, p, pos[p], Wt);
     R v[8], lim[4];
     line8<R, R>(wk.Bh + (size_t)q * fs + x, sp, v);
 #pragma unroll
-    for (int u = 0; u < 4; u++) lim[u] = (R)B[q * fs + (u - 2) * sp];
+    for (int u = 0; u < 4; u++) lim[u] = B[q * fs + (u - 2) * sp];
     recon_lr<R>(v, lim, Wt, a1, a2, bql, bqr);
   }
   const R bp = R(0.5) * (bpl + bpr), bq = R(0.5) * (bql + bqr);
@@ -323,10 +339,9 @@ __device__ __forceinline__ void flux_body(const Params& P, const Work<R>& wk, Po
   const int f = D == 0 ? i : (D == 1 ? j : k);
   const long long x = lin(P, i, j, k), s = sd<D>(P);
   const size_t fs = P.fs;
-  const int cb = cur_buf(P);
-  const double* __restrict__ W = P.Wbuf[cb] + x;
+  const R* __restrict__ W = lim_w<R>(P, wk) + x;
   FaceWeights<R> Wt;
-  load_weights<R>(P, D, f, Wt);
+  load_weights<R>(wk.tab, P.tmax, D, f, Wt);
   const R a1 = (R)P.pdm_a1, a2 = (R)P.pdm_a2;
   R L[6], Rt[6], mL[3], mR[3];
 #pragma unroll
@@ -334,7 +349,7 @@ __device__ __forceinline__ void flux_body(const Params& P, const Work<R>& wk, Po
     R v[8], lim[4];
     line8<R, R>(wk.Wh + (size_t)m * fs + x, s, v);
 #pragma unroll
-    for (int u = 0; u < 4; u++) lim[u] = (R)W[m * fs + (u - 2) * s];
+    for (int u = 0; u < 4; u++) lim[u] = W[m * fs + (u - 2) * s];
     recon_lr<R>(v, lim, Wt, a1, a2, L[m], Rt[m]);
   }
 #pragma unroll
@@ -352,8 +367,7 @@ __device__ __forceinline__ void flux_body(const Params& P, const Work<R>& wk, Po
   const R csl = sqrt(gm * pl * irl), csr = sqrt(gm * pr * irr);
   // entropy channel: p_S = 0 everywhere unless a problem sets it; the
   // zero test only skips exact zeros
-  const R csel = sl == R(0) ? R(0) : sqrt(gm * sl * irl);
-  const R cser = sr == R(0) ? R(0) : sqrt(gm * sr * irr);
+
   const R btl = mL[0] * mL[0] + mL[1] * mL[1] + mL[2] * mL[2];
   const R btr = mR[0] * mR[0] + mR[1] * mR[1] + mR[2] * mR[2];
   const R val = sqrt(btl * irl), var = sqrt(btr * irr);
@@ -361,7 +375,6 @@ __device__ __forceinline__ void flux_body(const Params& P, const Work<R>& wk, Po
   const R ver = var * ca * rsq(var * var + ca2);
   const R vnl = L[V1 + D], vnr = Rt[V1 + D];
   const R vf = fmax(fabs(vnl) + sqrt(csl * csl + vel * vel), fabs(vnr) + sqrt(csr * csr + ver * ver));
-  const R vfe = fmax(fabs(vnl) + sqrt(csel * csel + vel * vel), fabs(vnr) + sqrt(cser * cser + ver * ver));
   R mol[3], mor[3];
 #pragma unroll
   for (int a = 0; a < 3; a++) {
@@ -371,8 +384,7 @@ __device__ __forceinline__ void flux_body(const Params& P, const Work<R>& wk, Po
   const R igm1 = (R)P.inv_gm1;
   const R el = R(0.5) * rl * (L[V1] * L[V1] + L[V2] * L[V2] + L[V3] * L[V3]) + pl * igm1;
   const R er = R(0.5) * rr * (Rt[V1] * Rt[V1] + Rt[V2] * Rt[V2] + Rt[V3] * Rt[V3]) + pr * igm1;
-  const R Sl = (sl == R(0) && rl > R(0)) ? sl : sl / pow(rl, gm1);
-  const R Sr = (sr == R(0) && rr > R(0)) ? sr : sr / pow(rr, gm1);
+
   R* o = wk.F + (size_t)(9 * D) * fs + x;
   o[0] = R(0.5) * (mol[D] + mor[D] - vf * (rr - rl));
 #pragma unroll
@@ -382,8 +394,19 @@ __device__ __forceinline__ void flux_body(const Params& P, const Work<R>& wk, Po
     o[(1 + a) * fs] = R(0.5) * u;
   }
   o[4 * fs] = R(0.5) * (el * vnl + pl * vnl + er * vnr + pr * vnr - vf * (er - el));
-  o[5 * fs] = R(0.5) * (Sl * vnl + Sr * vnr - vfe * (Sr - Sl));
-  const R bn = (R)P.Bbuf[cb][x + D * fs];
+  // entropy channel (p_S = 0 unless a problem sets it): with zero left and
+  // right states its flux is zero and the update leaves p_S at +0 either way
+  R fS = R(0);
+  if (sl != R(0) || sr != R(0)) {
+    const R csel = sl == R(0) ? R(0) : sqrt(gm * sl * irl);
+    const R cser = sr == R(0) ? R(0) : sqrt(gm * sr * irr);
+    const R vfe = fmax(fabs(vnl) + sqrt(csel * csel + vel * vel), fabs(vnr) + sqrt(cser * cser + ver * ver));
+    const R Sl = (sl == R(0) && rl > R(0)) ? sl : sl / pow(rl, gm1);
+    const R Sr = (sr == R(0) && rr > R(0)) ? sr : sr / pow(rr, gm1);
+    fS = R(0.5) * (Sl * vnl + Sr * vnr - vfe * (Sr - Sl));
+  }
+  o[5 * fs] = fS;
+  const R bn = lim_b<R>(P, wk)[x + D * fs];
   const R bq = (btl + btr) * (R)P.q_ca;
 #pragma unroll
   for (int a = 0; a < 3; a++) {

@@ -18,8 +18,13 @@ struct Work {
   R* V;    // 6 centre-to-edge first-sweep velocities (2 per edge direction)
   R* E;    // 3 edge EMFs
   R* F;    // 27 face fluxes (9 per direction)
+  R* Wl;   // FP32 path: 6 step-start primitives in R (the limiters' reference)
+  R* Bl;   // FP32 path: 3 step-start face fields in R
+  const R* tab;  // the per-axis tables in R (same layout as Params::tab)
 };
 constexpr int WORK_FIELDS = 6 + 3 + 3 + 3 + 6 + 3 + 27;
+// the FP32 path adds the R copies of the step-start state (Wl, Bl)
+constexpr int work_fields(bool mixed) { return WORK_FIELDS + (mixed ? 9 : 0); }
 
 int64_t launches();
 void count_launches(int64_t n);  // kernels run by graph replays
