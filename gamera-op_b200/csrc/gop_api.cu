@@ -609,7 +609,8 @@ int gop_prepare(gop_instance* h, int restart) {
 static const dim3 kBlockCandidates[] = {dim3(32, 4, 2), dim3(32, 8, 1), dim3(32, 1, 8),
                                         dim3(32, 2, 4),  dim3(64, 2, 2), dim3(64, 4, 1),
                                         dim3(64, 1, 4),  dim3(128, 2, 1), dim3(128, 1, 2),
-                                        dim3(32, 4, 1),  dim3(64, 2, 1), dim3(256, 1, 1)};
+                                        dim3(32, 4, 1),  dim3(64, 2, 1), dim3(256, 1, 1),
+                                        dim3(8, 32, 1),  dim3(8, 4, 8)};
 static const int kNumBlockCandidates = sizeof(kBlockCandidates) / sizeof(kBlockCandidates[0]);
 
 static int enqueue_steps(gop_instance* h, int nsteps, double time_stop) {

@@ -234,16 +234,21 @@ __device__ __forceinline__ void ab2_body(const Params& P, const Work<R>& w, Pos 
 // First centre-to-edge sweep of center2corner_{jk,ki,ij}
 // (src/solver_func.c:686-778): for edges along D, velocity components
 // p=(D+1)%3 and q=(D+2)%3 reconstructed along p (limiter on the step-start
-// velocity) and averaged.  Points: D active, p faces lo..hi+1, q all ghosts.
+// velocity) and averaged, at D active, p faces lo..hi+1, q over all cells
+// including ghosts.  Over the active q range these are exactly the
+// velocity states the face flux along p reconstructs (same inputs, same
+// weights), so the flux stage writes them there and this kernel covers only
+// the 2*NGH ghost layers of q.
 template <typename R, int D>
 __device__ __forceinline__ void c2c_body(const Params& P, const Work<R>& wk, Pos t) {
   constexpr int p = (D + 1) % 3, q = (D + 2) % 3;
-  const int ijk[3] = {t.x, t.y, t.z};
+  int ijk[3] = {t.x, t.y, t.z};
   int cnt[3], lo[3];
   lo[D] = NGH; cnt[D] = P.n[D];
   lo[p] = NGH; cnt[p] = P.n[p] + 1;
-  lo[q] = 0;   cnt[q] = P.n[q] + 2 * NGH;
+  lo[q] = 0;   cnt[q] = 2 * NGH;
   if (ijk[0] >= cnt[0] || ijk[1] >= cnt[1] || ijk[2] >= cnt[2]) return;
+  if (ijk[q] >= NGH) ijk[q] += P.n[q];  // upper ghost layers
   const int i = ijk[0] + lo[0], j = ijk[1] + lo[1], k = ijk[2] + lo[2];
   const int f = p == 0 ? i : (p == 1 ? j : k);
   const long long x = lin(P, i, j, k), s = sd<p>(P);
@@ -385,6 +390,13 @@ __device__ __forceinline__ void flux_body(const Params& P, const Work<R>& wk, Po
   const R el = R(0.5) * rl * (L[V1] * L[V1] + L[V2] * L[V2] + L[V3] * L[V3]) + pl * igm1;
   const R er = R(0.5) * rr * (Rt[V1] * Rt[V1] + Rt[V2] * Rt[V2] + Rt[V3] * Rt[V3]) + pr * igm1;
 
+  // the first centre-to-edge sweep for edges along E = (D+2)%3: velocity
+  // components D and (D+1)%3 along D, averaged (see c2c_body)
+  {
+    constexpr int E = (D + 2) % 3, c1 = (D + 1) % 3;
+    wk.V[x + (size_t)(2 * E) * fs] = R(0.5) * (L[V1 + D] + Rt[V1 + D]);
+    wk.V[x + (size_t)(2 * E + 1) * fs] = R(0.5) * (L[V1 + c1] + Rt[V1 + c1]);
+  }
   R* o = wk.F + (size_t)(9 * D) * fs + x;
   o[0] = R(0.5) * (mol[D] + mor[D] - vf * (rr - rl));
 #pragma unroll
@@ -1088,8 +1100,10 @@ Tune::Tune() {
   // defaults: warps along i; the sweeps of D=1 / D=2 kernels run along the
   // block's longer transverse side so neighbouring rows share L1 lines
   for (int t = 0; t < NTUNE; t++) blk[t] = dim3(32, 4, 2);
-  blk[K_C2C1] = blk[K_EMF1] = blk[K_FLUX1] = dim3(32, 8, 1);
+  blk[K_EMF1] = blk[K_FLUX1] = dim3(32, 8, 1);
   blk[K_C2C2] = blk[K_EMF2] = blk[K_FLUX2] = dim3(32, 1, 8);
+  // the first edge sweep of edges along j covers only the 8 ghost layers of i
+  blk[K_C2C1] = dim3(8, 32, 1);
 }
 
 dim3 launch_space(const Params& P, int slot) {
@@ -1106,10 +1120,10 @@ dim3 launch_space(const Params& P, int slot) {
   const int stage = (slot - K_C2C0) / 3, D = (slot - K_C2C0) % 3;
   const int p = (D + 1) % 3, q = (D + 2) % 3;
   int cnt[3];
-  if (stage == 0) {
+  if (stage == 0) {  // ghost layers of q only (the flux stage covers the rest)
     cnt[D] = P.n[D];
     cnt[p] = P.n[p] + 1;
-    cnt[q] = P.n[q] + 2 * NGH;
+    cnt[q] = 2 * NGH;
   } else if (stage == 1) {
     cnt[D] = P.n[D];
     cnt[p] = P.n[p] + 1;
@@ -1169,7 +1183,8 @@ void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t
   hook(G_AB2, 1);
   launch_slot<R>(P, coord, w, K_AB2, tune.blk[K_AB2], st);
   hook(G_AB2, 0);
-  for (int stage = 0; stage < 3; stage++) {
+  // flux first: it also writes the edge velocities of the active range
+  for (int stage : {2, 0, 1}) {
     const int g = stage == 0 ? G_C2C : (stage == 1 ? G_EMF : G_FLUX);
     hook(g, 1);
     for (int d = 0; d < 3; d++) {
@@ -1250,8 +1265,11 @@ template <typename R>
 void launch_batch_step(const Member<R>* m, int n, const BatchLists& L, cudaStream_t st) {
   const int nb = (n + 127) / 128;
   LAUNCH(kb_begin<R>, nb, 128, st, m, n);
-  // the stages in step order; the ghost fill after both updates
-  for (int slot = 0; slot <= K_UPDATE; slot++)
+  // the stages in step order (flux before the first edge sweep, which it
+  // partly computes); the ghost fill after both updates
+  static const int order[] = {K_AB2, K_FLUX0, K_FLUX1, K_FLUX2, K_C2C0, K_C2C1, K_C2C2,
+                              K_EMF0, K_EMF1, K_EMF2, K_UPDATE};
+  for (int slot : order)
     launch_batch_slot<R>(m, slot, L.count[slot], L.blk[slot], L.items[slot], st);
   launch_batch_slot<R>(m, K_UPDATE_SPH, L.count[K_UPDATE_SPH], L.blk[K_UPDATE_SPH],
                        L.items[K_UPDATE_SPH], st);

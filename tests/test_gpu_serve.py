@@ -79,7 +79,7 @@ def test_batch_autotune_keeps_state_and_results(gop):
     members = [workloads.build(j) for j in jobs]
     b = gop.Batch(members)
     chosen = b.autotune(reps=1)
-    assert len(chosen) == 11 and all(0 <= v < 12 for v in chosen.values())
+    assert len(chosen) == 11 and all(0 <= v < 14 for v in chosen.values())
     b.step([j.steps for j in jobs])
     for a, m in zip(alone, members):
         d = m.download(("gas", "face_b"))
