@@ -404,7 +404,7 @@ def bench_batched(args, gop, torch, dist, rank, world, local, max_all, barrier):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
         "config": {"workload": f"batched_uneven_{len(jobs)}_mixed", "members": len(jobs),
                    "grids": {"x".join(map(str, k)): v for k, v in sorted(Counter(j.n for j in jobs).items())},
-                   "cells": sum(j.cells for j in jobs), "steps_per_member": K, "seed": 96,
+                   "cells": sum(j.cells for j in jobs), "steps_per_member": K, "seed": 20261203,
                    "parallelism": f"members sharded over {world} GPU(s), no data-path collective",
                    "l2": "states total tens of GB >> 126 MB L2, no flush needed",
                    "block_shapes": {k: BLOCK_CANDIDATES[v] for k, v in tuned.items()}},
@@ -435,7 +435,8 @@ def bench_served(args, gop, torch, dist, rank, world, local, max_all, barrier):
     barrier()
     launches0 = gop.kernel_launches()
     clocks = ClockSampler(local)
-    rep = serve.Server(eng, 150 * 10 ** 9, max_live=args.max_live, chunk=50).run(mine)
+    rep = serve.Server(eng, 150 * 10 ** 9, max_live=args.max_live, chunk=50,
+                       workers=4).run(mine)
     clk = clocks.stop()
     launches = gop.kernel_launches() - launches0
     eng.close()
@@ -467,7 +468,7 @@ def bench_served(args, gop, torch, dist, rank, world, local, max_all, barrier):
                    "rate_per_s": 50, "seed": 5150,
                    "grids": {"x".join(map(str, k)): v for k, v in sorted(Counter(j.n for j in jobs).items())},
                    "steps": "uniform [100, 1000]", "hbm_budget_gb": 150, "max_live": args.max_live,
-                   "round_steps": 50, "tolerance": 1e-5,
+                   "round_steps": 50, "host_workers": 4, "tolerance": 1e-5,
                    "parallelism": f"requests sharded over {world} GPU(s), no data-path collective",
                    "l2": "live states >> 126 MB L2"},
         "latency_s": {"p50": round(served["p50_s"], 3), "p99": round(served["p99_s"], 3),
@@ -476,6 +477,8 @@ def bench_served(args, gop, torch, dist, rank, world, local, max_all, barrier):
         "plain_fp64_one_at_a_time": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in base.items()},
         "speedup_vs_plain_fp64": round(served["mcell_updates_per_s"] / base["mcell_updates_per_s"], 3),
         "rounds": rep.rounds, "peak_live": rep.peak_live, "peak_bytes": rep.peak_bytes,
+        "host_seconds": {k: round(v, 3) for k, v in rep.seconds.items()},
+        "engine": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in eng.stats.items()},
         "accuracy_vs_fp64": {"max_rel_l1": worst[0], "variable": worst[1], "max_divb": divb,
                              "sampled_requests": len(kept), "tolerance": 1e-5},
         "gpu_launches": int(launches), "clocks": clk,

@@ -320,14 +320,15 @@ Layout layout_of(const gop_desc* d) {
 struct gop_instance {
   gop_desc d;
   Params P;
-  cudaStream_t st = nullptr;
+  cudaStream_t own = nullptr;  // the instance's own non-blocking stream
+  cudaStream_t st = nullptr;   // where its work goes (own, or the caller's)
   double* state = nullptr;   // 2 x (6 + 3) fields
   void* work = nullptr;      // WORK_FIELDS x R
   double* tab = nullptr;
   float* tabf = nullptr;     // FP32 copy of the tables (mixed path)
   double* scal = nullptr;
   double* staging = nullptr; // reference-layout scratch, 6 x NI*NJ*NK
-  double* hscal = nullptr;   // pinned host copy of the scalars
+  double* hscal = nullptr;   // host copy of the scalars
   Work<double> wd;
   Work<float> wf;
   Tune tune;
@@ -454,12 +455,14 @@ int gop_create(const gop_desc* desc, gop_instance** out) {
 
   size_t rsize = d.precision == GOP_PREC_MIXED ? sizeof(float) : sizeof(double);
   size_t ref = (size_t)L.N[0] * L.N[1] * L.N[2];
-  cudaError_t e = cudaSuccess;
-  // stream-ordered allocations: creating and destroying instances does not
-  // wait for work of other instances or batches running on other streams
+  // Every instance works on its own non-blocking stream with stream-ordered
+  // allocations, so creating, using and destroying one instance never waits
+  // for another instance or a batch (the legacy default stream would).
+  cudaError_t e = cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking);
+  h->st = h->own;
   auto alloc = [&](void** p, size_t bytes) {
     if (e == cudaSuccess) {
-      e = cudaMallocAsync(p, bytes, 0);
+      e = cudaMallocAsync(p, bytes, h->st);
       if (e == cudaSuccess) h->bytes += bytes;
     }
   };
@@ -475,21 +478,22 @@ int gop_create(const gop_desc* desc, gop_instance** out) {
     h->hscal = new (std::nothrow) double[NSCAL];
     if (!h->hscal) e = cudaErrorMemoryAllocation;
   }
-  if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
   if (e != cudaSuccess) {
     cudaGetLastError();
     gop_destroy(h);
     return fail(GOP_ENOMEM, "device allocation of %zu bytes failed: %s", gop_footprint(&d),
                 cudaGetErrorString(e));
   }
-  cudaMemset(h->state, 0, (size_t)L.fs * 18 * sizeof(double));
-  cudaMemset(h->work, 0, (size_t)L.fs * nwork * rsize);
-  cudaMemcpy(h->tab, T.v.data(), T.v.size() * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemsetAsync(h->state, 0, (size_t)L.fs * 18 * sizeof(double), h->st);
+  cudaMemsetAsync(h->work, 0, (size_t)L.fs * nwork * rsize, h->st);
+  cudaMemcpyAsync(h->tab, T.v.data(), T.v.size() * sizeof(double), cudaMemcpyHostToDevice, h->st);
+  std::vector<float> tf;
   if (mixed) {
-    std::vector<float> tf(T.v.begin(), T.v.end());
-    cudaMemcpy(h->tabf, tf.data(), tf.size() * sizeof(float), cudaMemcpyHostToDevice);
+    tf.assign(T.v.begin(), T.v.end());
+    cudaMemcpyAsync(h->tabf, tf.data(), tf.size() * sizeof(float), cudaMemcpyHostToDevice, h->st);
   }
-  cudaMemset(h->scal, 0, NSCAL * sizeof(double));
+  cudaMemsetAsync(h->scal, 0, NSCAL * sizeof(double), h->st);
   P.tab = h->tab;
   P.scal = h->scal;
   P.Wbuf[0] = h->state;
@@ -505,9 +509,7 @@ int gop_create(const gop_desc* desc, gop_instance** out) {
     h->wd = Work<double>{w, w + 6 * L.fs, w + 9 * L.fs, w + 12 * L.fs, w + 15 * L.fs,
                          w + 21 * L.fs, w + 24 * L.fs, nullptr, nullptr, h->tab};
   }
-  // the set-up above ran on the legacy default stream; work of batches on
-  // their own (non-blocking) streams keeps running meanwhile
-  cudaError_t le = cudaStreamSynchronize(0);
+  cudaError_t le = cudaStreamSynchronize(h->st);
   if (le == cudaSuccess) le = cudaGetLastError();
   if (le != cudaSuccess) {
     gop_destroy(h);
@@ -519,10 +521,11 @@ int gop_create(const gop_desc* desc, gop_instance** out) {
 
 int gop_destroy(gop_instance* h) {
   if (!h) return GOP_OK;
-  cudaStreamSynchronize(h->st);
+  if (h->st) cudaStreamSynchronize(h->st);
   for (void* p : {(void*)h->state, h->work, (void*)h->tab, (void*)h->tabf, (void*)h->scal,
                   (void*)h->staging})
     if (p) cudaFreeAsync(p, h->st);
+  if (h->own) cudaStreamDestroy(h->own);  // released once the frees have run
   delete[] h->hscal;
   prof_collect(h);
   for (cudaEvent_t e : h->pool) cudaEventDestroy(e);
@@ -532,7 +535,8 @@ int gop_destroy(gop_instance* h) {
 
 int gop_set_stream(gop_instance* h, void* stream) {
   if (!h) return fail(GOP_EINVAL, "instance is NULL");
-  h->st = (cudaStream_t)stream;
+  CK(cudaStreamSynchronize(h->st));
+  h->st = stream ? (cudaStream_t)stream : h->own;
   return GOP_OK;
 }
 
@@ -951,21 +955,24 @@ static int batch_build(gop_batch* b) {
     return fail(GOP_ENOMEM, "batch allocation of %zu bytes failed: %s", off, cudaGetErrorString(e));
   }
   char* base = (char*)b->dev;
-  CK(cudaMemcpy(base + o_mem[0], md.data(), md.size() * sizeof(Member<double>), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(base + o_mem[1], mf.data(), mf.size() * sizeof(Member<float>), cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(base + o_mem[0], md.data(), md.size() * sizeof(Member<double>),
+                     cudaMemcpyHostToDevice, b->own));
+  CK(cudaMemcpyAsync(base + o_mem[1], mf.data(), mf.size() * sizeof(Member<float>),
+                     cudaMemcpyHostToDevice, b->own));
   for (int s = 0; s < 2; s++) {
     BatchSide& S = b->side[s];
     S.n = (int)b->idx[s].size();
     S.members = base + o_mem[s];
     S.steps = (int*)(base + o_steps[s]);
     for (int slot = 0; slot < NSLOT; slot++) {
-      CK(cudaMemcpy(base + o_items[s][slot], items[s][slot].data(), items[s][slot].size() * 8,
-                    cudaMemcpyHostToDevice));
+      CK(cudaMemcpyAsync(base + o_items[s][slot], items[s][slot].data(), items[s][slot].size() * 8,
+                         cudaMemcpyHostToDevice, b->own));
       S.L.count[slot] = (int)items[s][slot].size();
       S.L.blk[slot] = batch_block(b, slot);
       S.L.items[slot] = (const unsigned long long*)(base + o_items[s][slot]);
     }
   }
+  CK(cudaStreamSynchronize(b->own));  // the host images above go out of scope
   cudaGraph_t g = nullptr;
   const int64_t before = launches();
   CK(cudaStreamBeginCapture(b->own, cudaStreamCaptureModeThreadLocal));
@@ -1054,7 +1061,8 @@ int gop_batch_autotune(gop_batch* b, int reps, int* chosen) {
   std::vector<std::vector<double>> saved(b->m.size());
   for (size_t i = 0; i < b->m.size(); i++) {
     gop_instance* h = b->m[i];
-    CK(cudaMemcpy(h->hscal, h->scal, NSCAL * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpyAsync(h->hscal, h->scal, NSCAL * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
     saved[i].assign(h->hscal, h->hscal + NSCAL);
     if (saved[i][S_PAR] != 0.0) return fail(GOP_ESTATE, "member %zu is not freshly prepared", i);
   }
@@ -1090,7 +1098,8 @@ int gop_batch_autotune(gop_batch* b, int reps, int* chosen) {
           ok = false;
           break;
         }
-        if (cudaMemcpy(ditems, items.data(), items.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess) {
+        if (cudaMemcpyAsync(ditems, items.data(), items.size() * 8, cudaMemcpyHostToDevice,
+                            b->own) != cudaSuccess) {
           rc = fail(GOP_ECUDA, "autotune upload failed");
           ok = false;
           break;
@@ -1127,10 +1136,13 @@ int gop_batch_autotune(gop_batch* b, int reps, int* chosen) {
   for (size_t i = 0; i < b->m.size(); i++) {
     gop_instance* h = b->m[i];
     const Params& P = h->P;
-    CK(cudaMemcpy(P.Wbuf[1], P.Wbuf[0], (size_t)P.fs * 6 * sizeof(double), cudaMemcpyDeviceToDevice));
-    CK(cudaMemcpy(P.Bbuf[1], P.Bbuf[0], (size_t)P.fs * 3 * sizeof(double), cudaMemcpyDeviceToDevice));
+    CK(cudaMemcpyAsync(P.Wbuf[1], P.Wbuf[0], (size_t)P.fs * 6 * sizeof(double),
+                       cudaMemcpyDeviceToDevice, b->own));
+    CK(cudaMemcpyAsync(P.Bbuf[1], P.Bbuf[0], (size_t)P.fs * 3 * sizeof(double),
+                       cudaMemcpyDeviceToDevice, b->own));
     for (int t = 0; t < NSCAL; t++) h->hscal[t] = saved[i][t];
-    CK(cudaMemcpy(h->scal, h->hscal, NSCAL * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(h->scal, h->hscal, NSCAL * sizeof(double), cudaMemcpyHostToDevice, b->own));
+    CK(cudaStreamSynchronize(b->own));
   }
   if (rc) return rc;
   return batch_build(b);
@@ -1169,7 +1181,8 @@ int gop_batch_wait(gop_batch* b) {
   CK(cudaGetLastError());
   for (gop_instance* h : b->m) {
     double* sc = h->hscal;
-    CK(cudaMemcpy(sc, h->scal, NSCAL * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpyAsync(sc, h->scal, NSCAL * sizeof(double), cudaMemcpyDeviceToHost, b->st));
+    CK(cudaStreamSynchronize(b->st));
     if (sc[S_FLAGS] != 0.0) return fail(GOP_ENUMERIC, "non-finite or non-positive state in a member");
   }
   return GOP_OK;

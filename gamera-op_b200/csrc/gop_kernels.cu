@@ -27,6 +27,7 @@
 #include "gop_device.cuh"
 #include "gop_kernels.h"
 
+#include <atomic>
 #include <cfloat>
 
 namespace gop {
@@ -1082,8 +1083,9 @@ __global__ void k_mags(Params P, const double* __restrict__ B, double* __restric
 
 // ----------------------------------------------------------- launchers
 
-static int64_t g_launches = 0;
-int64_t launches() { return g_launches; }
+// launches by this process (any host thread)
+static std::atomic<int64_t> g_launches{0};
+int64_t launches() { return g_launches.load(); }
 void count_launches(int64_t n) { g_launches += n; }
 
 static dim3 grid3(int a, int b, int c, dim3 blk) {

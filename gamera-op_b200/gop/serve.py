@@ -23,8 +23,10 @@ Time-to-solution of a request is its completion time minus its arrival time
 """
 from __future__ import annotations
 
+import threading
 import time
 from collections import deque
+from concurrent.futures import FIRST_COMPLETED, Future, ThreadPoolExecutor, wait
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -56,6 +58,10 @@ class ServeReport:
     rounds: int = 0
     peak_live: int = 0
     peak_bytes: int = 0
+    # host seconds by activity (launch includes building a batch that was
+    # not prebuilt; wait is the host blocked on the round)
+    seconds: dict = field(default_factory=lambda: dict(launch=0.0, retire=0.0, admit=0.0,
+                                                       prebuild=0.0, wait=0.0, idle=0.0))
 
     def cell_updates(self) -> int:
         return sum(o.cells * o.steps for o in self.outcomes)
@@ -66,6 +72,7 @@ class ServeReport:
     def summary(self) -> dict:
         return dict(requests=len(self.outcomes), makespan_s=self.makespan, rounds=self.rounds,
                     peak_live=self.peak_live, peak_bytes=self.peak_bytes,
+                    host_seconds={k: round(v, 3) for k, v in self.seconds.items()},
                     mcell_updates_per_s=self.cell_updates() / self.makespan / 1e6,
                     p50_s=self.latency(50), p99_s=self.latency(99))
 
@@ -74,11 +81,14 @@ class Server:
     """Admission by slots and HBM budget, resident state, batched rounds."""
 
     def __init__(self, engine, hbm_budget: int, max_live: int = 32, chunk: int = 50,
-                 clock=time.perf_counter, sleep=time.sleep):
+                 clock=time.perf_counter, sleep=time.sleep, workers: int = 0):
+        """``workers`` > 0 runs request set-up (``create``) and result
+        copy-back (``finish``) on that many host threads, so neither holds
+        up the loop that feeds the GPU; 0 runs them inline."""
         if chunk <= 0 or max_live <= 0:
             raise ValueError("chunk and max_live must be positive")
         self.engine, self.budget, self.max_live, self.chunk = engine, int(hbm_budget), max_live, chunk
-        self.clock, self.sleep = clock, sleep
+        self.clock, self.sleep, self.workers = clock, sleep, int(workers)
 
     def run(self, jobs) -> ServeReport:
         eng = self.engine
@@ -87,19 +97,36 @@ class Server:
             if eng.footprint(j) > self.budget:
                 raise AdmissionError(f"request {j.rid} needs {eng.footprint(j)} bytes, "
                                      f"more than the budget of {self.budget}")
+        pool = ThreadPoolExecutor(self.workers) if self.workers > 0 else None
         rep = ServeReport()
-        live = []     # [job, handle, remaining, outcome]: in the next / current round
-        ready = []    # admitted while a round runs: join the next one
-        done = []     # finished, result not yet copied back
+        sec = rep.seconds
+        starting = []  # [job, future of handle, outcome]: being set up
+        ready = []     # [job, handle, remaining, outcome]: join the next round
+        live = []      # in the next / current round
+        leaving = []   # [job, future of result, outcome]: result being copied back
         used = 0
         t0 = self.clock()
 
         def now():
             return self.clock() - t0
 
+        def timed(key, fn, *a):
+            t = self.clock()
+            r = fn(*a)
+            sec[key] += self.clock() - t
+            return r
+
+        def run_async(fn, *a):
+            if pool is not None:
+                return pool.submit(fn, *a)
+            f = Future()
+            f.set_result(fn(*a))
+            return f
+
         def admit():
             nonlocal used
-            while pending and pending[0].arrival <= now() and len(live) + len(ready) < self.max_live:
+            while (pending and pending[0].arrival <= now()
+                   and len(live) + len(ready) + len(starting) < self.max_live):
                 j = pending[0]
                 fp = eng.footprint(j)
                 if used + fp > self.budget:
@@ -107,43 +134,59 @@ class Server:
                 pending.popleft()
                 out = Outcome(j.rid, j.arrival, admitted=now(), cells=j.cells, steps=j.steps)
                 used += fp
-                ready.append([j, eng.create(j), j.steps, out])
-                rep.peak_live = max(rep.peak_live, len(live) + len(ready))
+                starting.append([j, run_async(eng.create, j), out])
+                rep.peak_live = max(rep.peak_live, len(live) + len(ready) + len(starting))
                 rep.peak_bytes = max(rep.peak_bytes, used)
 
-        def retire():
+        def collect(block=False):
+            """Moves set-up and copy-back work that has finished along."""
             nonlocal used
-            while done:
-                j, h, _, out = done.pop(0)
-                out.result = eng.finish(j, h)
+            if block and not any(e[1].done() for e in starting + leaving):
+                wait([e[1] for e in starting + leaving], return_when=FIRST_COMPLETED)
+            for e in [e for e in starting if e[1].done()]:
+                starting.remove(e)
+                ready.append([e[0], e[1].result(), e[0].steps, e[2]])
+            for e in [e for e in leaving if e[1].done()]:
+                leaving.remove(e)
+                j, f, out = e
+                out.result = f.result()
                 out.done = now()
                 used -= eng.footprint(j)
                 rep.outcomes.append(out)
 
-        while pending or live or ready or done:
-            live += ready
-            ready.clear()
-            if not live:
-                retire()
-                admit()
-                if not ready and pending and pending[0].arrival > now():
-                    self.sleep(pending[0].arrival - now())  # idle until the next arrival
-                continue
-            steps = [min(self.chunk, e[2]) for e in live]
-            eng.launch([e[1] for e in live], steps)
-            rep.rounds += 1
-            # while the round runs: results of the last round go back, freed
-            # memory and slots take new requests, the next round is prepared
-            retire()
-            admit()
-            nxt = [e[1] for e, s in zip(live, steps) if e[2] > s] + [e[1] for e in ready]
-            if nxt:
-                eng.prebuild(nxt)
-            eng.wait()
-            for e, s in zip(live, steps):
-                e[2] -= s
-            done += [e for e in live if e[2] == 0]
-            live = [e for e in live if e[2] > 0]
+        try:
+            while pending or live or ready or starting or leaving:
+                timed("admit", collect)
+                timed("admit", admit)
+                live += ready
+                ready.clear()
+                if not live:
+                    if starting or leaving:
+                        timed("idle", collect, True)
+                    elif pending and pending[0].arrival > now():
+                        # idle until the next arrival
+                        timed("idle", self.sleep, pending[0].arrival - now())
+                    continue
+                steps = [min(self.chunk, e[2]) for e in live]
+                timed("launch", eng.launch, [e[1] for e in live], steps)
+                rep.rounds += 1
+                # while the round runs: new arrivals are set up, the next
+                # round's batch is prepared
+                timed("admit", collect)
+                timed("admit", admit)
+                nxt = [e[1] for e, s in zip(live, steps) if e[2] > s] + [e[1] for e in ready]
+                if nxt:
+                    timed("prebuild", eng.prebuild, nxt)
+                timed("wait", eng.wait)
+                for e, s in zip(live, steps):
+                    e[2] -= s
+                for e in live:
+                    if e[2] == 0:
+                        leaving.append([e[0], run_async(eng.finish, e[0], e[1]), e[3]])
+                live = [e for e in live if e[2] > 0]
+        finally:
+            if pool is not None:
+                pool.shutdown(wait=True)
         rep.makespan = now()
         rep.outcomes.sort(key=lambda o: o.rid)
         return rep
@@ -183,8 +226,7 @@ class GpuEngine:
         self._batch, self._members = None, ()
         self._next, self._next_members = None, ()
         self._fp = {}
-        self._host = {}   # result buffers per grid shape
-        self._init = {}   # initial-state buffers per grid shape
+        self.stats = dict(builds=0, build_s=0.0, prebuilt_used=0, launch_s=0.0)
 
     def footprint(self, job):
         key = (job.n, job.precision if self.precision is None else self.precision)
@@ -192,15 +234,27 @@ class GpuEngine:
             self._fp[key] = self._wl.footprint(job, self.precision)
         return self._fp[key]
 
+    def _buffers(self, name):
+        # host buffers per worker thread (set-up and copy-back may run on
+        # several threads at once)
+        return self.__dict__.setdefault(f"{name}_{threading.get_ident()}", {})
+
     def create(self, job):
-        return self._wl.build(job, self.precision, host=self._init)
+        return self._wl.build(job, self.precision, host=self._buffers("init"))
+
+    def _build(self, members):
+        t = time.perf_counter()
+        b = self._Batch(members)
+        self.stats["builds"] += 1
+        self.stats["build_s"] += time.perf_counter() - t
+        return b
 
     def prebuild(self, handles):
         members = tuple(handles)
         if members not in (self._members, self._next_members):
             if self._next is not None:
                 self._next.close()
-            self._next, self._next_members = self._Batch(members), members
+            self._next, self._next_members = self._build(members), members
 
     def launch(self, handles, steps):
         members = tuple(handles)
@@ -210,15 +264,18 @@ class GpuEngine:
             if members == self._next_members:
                 self._batch, self._members = self._next, members
                 self._next, self._next_members = None, ()
+                self.stats["prebuilt_used"] += 1
             else:
-                self._batch, self._members = self._Batch(members), members
+                self._batch, self._members = self._build(members), members
+        t = time.perf_counter()
         self._batch.launch(steps)
+        self.stats["launch_s"] += time.perf_counter() - t
 
     def wait(self):
         self._batch.wait()
 
     def finish(self, job, inst):
-        res = download_result(inst, self._host, copy=self.keep(job))
+        res = download_result(inst, self._buffers("host"), copy=self.keep(job))
         inst.close()
         return res
 

@@ -5,10 +5,10 @@ physics parameters, step count); ``build`` turns one into a prepared
 :class:`gop.Instance`.  The generators only use numpy's seeded
 ``default_rng``, so the same seed gives the same work on every machine.
 
-* ``batched_uneven``: independent Orszag-Tang / blast-wave grids of uneven
-  size, gamma in [1.4, 5/3], blast overpressure ratio in [10, 1000] and
-  background plasma beta in [0.01, 10] (both log-uniform), field direction
-  uniform on the sphere.
+* ``batched_uneven``: independent Orszag-Tang (thin grids) and blast-wave
+  (cubes) grids of uneven size, gamma in [1.4, 5/3], blast overpressure
+  ratio in [10, 1000] and background plasma beta in [0.01, 10] (uniform),
+  field direction uniform on the sphere.
 * ``served_stream``: a Poisson arrival stream of blast-wave and Cartesian
   field-loop requests with grid sizes drawn from fixed weights and step
   counts uniform in [100, 1000].
@@ -72,21 +72,24 @@ def _unit_vector(rng):
     return v / np.linalg.norm(v)
 
 
-def batched_uneven(count=96, steps=20, seed=96):
-    """Independent OT / blast grids of uneven size (sizes uniform over
-    BATCH_GRIDS), all advanced by ``steps`` steps."""
+def batched_uneven(count=96, steps=200, seed=20261203):
+    """Independent grids of uneven size (uniform over BATCH_GRIDS): the thin
+    n^2 x 4 grids hold an Orszag-Tang vortex, the cubes a blast wave with
+    overpressure ratio ~ U[10, 1000] over p_out = 0.1, plasma beta
+    2 p_out / |B|^2 ~ U[0.01, 10] and field direction uniform on the sphere;
+    gamma ~ U[1.4, 5/3] for all.  Every member advances ``steps`` steps."""
     rng = np.random.default_rng(seed)
     jobs = []
     for r in range(count):
         n = BATCH_GRIDS[rng.integers(len(BATCH_GRIDS))]
-        kind = PROBLEM_OT if rng.random() < 0.5 else PROBLEM_BLAST
+        kind = PROBLEM_OT if n[2] == 4 else PROBLEM_BLAST
         gamma = float(rng.uniform(1.4, 5.0 / 3.0))
         over = {}
         if kind == PROBLEM_BLAST:
-            ratio = float(10 ** rng.uniform(1.0, 3.0))
-            beta = float(10 ** rng.uniform(-2.0, 1.0))
+            ratio = float(rng.uniform(10.0, 1000.0))
+            beta = float(rng.uniform(0.01, 10.0))
             p_out = 0.1
-            bmag = math.sqrt(2.0 * p_out / beta)  # beta = p / (B^2 / 2)
+            bmag = math.sqrt(2.0 * p_out / beta)
             over = dict(p_out=p_out, p_in=ratio * p_out, b=tuple(bmag * _unit_vector(rng)))
         jobs.append(Job(r, kind, n, steps, gamma, over, _domain(kind, n)))
     return jobs

@@ -40,7 +40,7 @@ def test_served_results_equal_alone_and_within_tolerance_of_fp64(gop):
     jobs = _jobs(gop)
     eng = serve.GpuEngine(keep=lambda j: True)
     budget = 3 * max(eng.footprint(j) for j in jobs)
-    rep = serve.Server(eng, budget, max_live=3, chunk=16).run(jobs)
+    rep = serve.Server(eng, budget, max_live=3, chunk=16, workers=2).run(jobs)
     assert len(rep.outcomes) == len(jobs)
     assert rep.peak_bytes <= budget and rep.peak_live <= 3
     assert rep.rounds > max(j.steps for j in jobs) // 16  # requests shared rounds

@@ -195,3 +195,18 @@ def test_two_rank_sharded_serving_over_gloo():
     assert totals[0]["makespan_s"] == max(g[3] for g in got)
     jobs = served_stream(count=30, seed=4)
     assert totals[0]["cell_updates"] == sum(j.cells * j.steps for j in jobs)
+
+
+def test_threaded_set_up_and_copy_back_keep_the_invariants():
+    jobs = served_stream(count=50, seed=6)
+    clk = Clock()
+    eng = FakeEngine(clk)
+    eng.cells = {j.rid: j.cells for j in jobs}
+    budget = 3 * max(1000 * j.cells for j in jobs)
+    rep = serve.Server(eng, budget, max_live=6, chunk=40, clock=clk, sleep=clk.sleep,
+                       workers=3).run(jobs)
+    assert sorted(o.rid for o in rep.outcomes) == list(range(50))
+    for o in rep.outcomes:
+        assert o.result == next(j.steps for j in jobs if j.rid == o.rid)
+    assert rep.peak_bytes <= budget and rep.peak_live <= 6
+    assert not eng.live
