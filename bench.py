@@ -194,9 +194,12 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="blast256", choices=["blast256", "batched", "served"],
+    ap.add_argument("--workload", default="blast256",
+                    choices=["blast256", "batched", "served", "ot", "sphere"],
                     help="blast256: the single 256^3 grid (default); batched: 96 uneven "
-                         "OT/blast grids in one batch; served: a Poisson request stream")
+                         "OT/blast grids in one batch; served: a Poisson request stream; "
+                         "ot: Orszag-Tang 256x256x4 to t=0.5; sphere: field loop on a "
+                         "192x128x128 spherical shell for one crossing")
     ap.add_argument("--requests", type=int, default=160, help="served: stream length")
     ap.add_argument("--members", type=int, default=96, help="batched: number of grids")
     ap.add_argument("--max-live", type=int, default=32, help="served: live request slots")
@@ -232,7 +235,8 @@ def main():
 
     import gop
     if args.workload != "blast256":
-        fn = bench_batched if args.workload == "batched" else bench_served
+        fn = {"batched": bench_batched, "served": bench_served, "ot": bench_ot,
+              "sphere": bench_sphere}[args.workload]
         line = fn(args, gop, torch, dist, rank, world, local, max_all, barrier)
         if rank == 0:
             print(json.dumps(line))
@@ -483,6 +487,89 @@ def bench_served(args, gop, torch, dist, rank, world, local, max_all, barrier):
                              "sampled_requests": len(kept), "tolerance": 1e-5},
         "gpu_launches": int(launches), "clocks": clk,
     }
+
+
+def _run_to(gop, torch, inst, steps, time_stop):
+    """Advances an instance on a fresh stream, timed with CUDA events;
+    returns (device ms, steps taken)."""
+    stream = torch.cuda.Stream()
+    inst.set_stream(stream.cuda_stream)
+    s0 = inst.stats()["steps"]
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    inst.step(steps, time_stop=time_stop, sync=False)
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b), inst.stats()["steps"] - s0
+
+
+def _single_pair(args, gop, torch, local, make, n, t_end, workload, extra):
+    """FP64 to t_end, then the mixed path for the same number of steps; the
+    mixed result is compared with the FP64 one."""
+    from gop import accuracy
+    warm = make(gop.PREC_FP64)
+    warm.prepare()
+    warm.step(max(args.warmup, 3))
+    warm.close()
+    launches0 = gop.kernel_launches()
+    clocks = ClockSampler(local)
+    f64 = make(gop.PREC_FP64)
+    f64.prepare()
+    ms64, steps = _run_to(gop, torch, f64, 10 ** 8, t_end)
+    mx = make(gop.PREC_MIXED)
+    mx.prepare()
+    msmx, steps_mx = _run_to(gop, torch, mx, steps, 1e300)
+    clk = clocks.stop()
+    launches = gop.kernel_launches() - launches0
+    cells = n[0] * n[1] * n[2]
+    which = ("gas", "face_b", "mags")
+    a, b = mx.download(which), f64.download(which)
+    errs = accuracy.rel_l1(n, a, b)
+    sl = tuple(slice(4, 4 + m) for m in n)
+    bm = lambda d: np.sqrt(sum(d["mags"][c][sl] ** 2 for c in range(3)))
+    ba, bb = bm(a), bm(b)
+    l1_bmag = float(np.abs(ba - bb).sum() / max(np.abs(bb).sum(), 1e-300))
+    st64, stmx = f64.stats(), mx.stats()
+    rate = lambda ms, k: round(cells * k / (ms / 1e3) / 1e6, 3)
+    line = {
+        "metric": METRIC, "value": rate(msmx, steps_mx), "unit": UNIT, "n_gpus": 1,
+        "steps": steps, "warmup": max(args.warmup, 3), "ms_per_step": round(msmx / steps_mx, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic",
+        "config": dict(workload=workload, grid=list(n), t_end=t_end,
+                       l2="state >> 126 MB L2" if cells >= 2 ** 20 else "state fits L2 (small grid)",
+                       **extra),
+        "plain_fp64": {"value": rate(ms64, steps), "ms_per_step": round(ms64 / steps, 4),
+                       "time": st64["time"], "divb_max": st64["divb_max"]},
+        "speedup_vs_plain_fp64": round(rate(msmx, steps_mx) / rate(ms64, steps), 3),
+        "accuracy_vs_fp64": {"rel_l1": errs, "l1_bmag": l1_bmag, "l1_rho": errs["rho"],
+                             "max_divb_mixed": stmx["divb_max"], "time_mixed": stmx["time"],
+                             "tolerance": 1e-5},
+        "gpu_launches": int(launches), "clocks": clk,
+    }
+    f64.close()
+    mx.close()
+    return line
+
+
+def bench_ot(args, gop, torch, dist, rank, world, local, max_all, barrier):
+    """Orszag-Tang vortex, 256x256x4 periodic, FP64 to t = 0.5 (the last
+    step overshoots, as in the reference), mixed for the same steps."""
+    n = (256, 256, 4)
+    make = lambda prec: gop.make(gop.PROBLEM_OT, n, domain=(0, 1, 0, 1, 0, 1 / 64), precision=prec)
+    return _single_pair(args, gop, torch, local, make, n, 0.5, "orszag_tang_256x256x4_to_t0.5",
+                        {"problem": "OT rho=25/(36pi) p=5/(12pi) gamma=5/3 CFL=0.3"})
+
+
+def bench_sphere(args, gop, torch, dist, rank, world, local, max_all, barrier):
+    """Field loop advected through a pole-free spherical shell r in [1,2],
+    theta in [pi/4, 3pi/4], phi in [-pi/4, pi/4], 192x128x128, outflow: FP64
+    for one crossing (t = 2.1), mixed for the same steps."""
+    n = (192, 128, 128)
+    make = lambda prec: gop.make(gop.PROBLEM_LOOP_SPH, n, bc="eeeeee", precision=prec)
+    return _single_pair(args, gop, torch, local, make, n, 2.1, "field_loop_sphere_192x128x128_one_crossing",
+                        {"problem": "loop R=0.15 at (1.5,0,0), A0=1e-3, v=(0,1,0.5), rho=1 p=1"})
 
 
 def measure_e2e(gop, torch, n, prec, args, max_all, barrier, world):

@@ -332,6 +332,8 @@ struct gop_instance {
   Work<double> wd;
   Work<float> wf;
   Tune tune;
+  cudaGraphExec_t step_graph = nullptr;  // one captured step (replayed by gop_step)
+  int64_t step_nodes = 0;
   size_t bytes = 0;
   bool prepared = false;
   bool fresh = false;  // prepared without restart and not stepped: history == state
@@ -382,6 +384,11 @@ static void prof_collect(gop_instance* h) {
     h->pool.push_back(r.b);
   }
   h->recs.clear();
+}
+
+static void drop_step_graph(gop_instance* h) {
+  if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
+  h->step_graph = nullptr;
 }
 
 extern "C" {
@@ -522,6 +529,7 @@ int gop_create(const gop_desc* desc, gop_instance** out) {
 int gop_destroy(gop_instance* h) {
   if (!h) return GOP_OK;
   if (h->st) cudaStreamSynchronize(h->st);
+  drop_step_graph(h);
   for (void* p : {(void*)h->state, h->work, (void*)h->tab, (void*)h->tabf, (void*)h->scal,
                   (void*)h->staging})
     if (p) cudaFreeAsync(p, h->st);
@@ -617,6 +625,49 @@ static const dim3 kBlockCandidates[] = {dim3(32, 4, 2), dim3(32, 8, 1), dim3(32,
                                         dim3(8, 32, 1),  dim3(8, 4, 8)};
 static const int kNumBlockCandidates = sizeof(kBlockCandidates) / sizeof(kBlockCandidates[0]);
 
+// one step's launches: begin, the stages, the ghost fill, end
+static void enqueue_one_step(gop_instance* h, cudaStream_t st, const Hook& hook) {
+  const Params& P = h->P;
+  hook(G_BEGIN, 1);
+  launch_begin(P, st);
+  hook(G_BEGIN, 0);
+  if (h->d.precision == GOP_PREC_MIXED)
+    launch_step_body<float>(P, h->d.coord, h->wf, st, h->tune, hook);
+  else
+    launch_step_body<double>(P, h->d.coord, h->wd, st, h->tune, hook);
+  hook(G_GHOST, 1);
+  launch_ghosts(P, h->d.bc, h->d.gem_bc, 0, st);
+  hook(G_GHOST, 0);
+  hook(G_END, 1);
+  launch_end(P, st);
+  hook(G_END, 0);
+}
+
+// Captures one step as a CUDA graph: every launch reads dt, the AB2
+// coefficient, the buffer parity and the stop flag from device memory, so
+// the same graph replays every step.
+static int capture_step(gop_instance* h) {
+  if (h->step_graph) return GOP_OK;
+  CK(cudaStreamSynchronize(h->own));
+  cudaGraph_t g = nullptr;
+  const int64_t before = launches();
+  CK(cudaStreamBeginCapture(h->own, cudaStreamCaptureModeThreadLocal));
+  enqueue_one_step(h, h->own, Hook());
+  cudaError_t e = cudaStreamEndCapture(h->own, &g);
+  h->step_nodes = launches() - before;
+  count_launches(-h->step_nodes);  // counted when replayed
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&h->step_graph, g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    h->step_graph = nullptr;
+    return fail(GOP_ECUDA, "step graph capture failed: %s", cudaGetErrorString(e));
+  }
+  return GOP_OK;
+}
+
+// steps between looks at the stop flag when gop_step runs to a stop time
+static const int kStopCheck = 256;
+
 static int enqueue_steps(gop_instance* h, int nsteps, double time_stop) {
   const Params& P = h->P;
   if (nsteps > 0) h->fresh = false;
@@ -626,21 +677,25 @@ static int enqueue_steps(gop_instance* h, int nsteps, double time_stop) {
     hook.ctx = h;
   }
   launch_arm(P, time_stop, (double)nsteps, h->st);
-  for (int n = 0; n < nsteps; n++) {
-    hook(G_BEGIN, 1);
-    launch_begin(P, h->st);
-    hook(G_BEGIN, 0);
-    if (h->d.precision == GOP_PREC_MIXED)
-      launch_step_body<float>(P, h->d.coord, h->wf, h->st, h->tune, hook);
-    else
-      launch_step_body<double>(P, h->d.coord, h->wd, h->st, h->tune, hook);
-    hook(G_GHOST, 1);
-    launch_ghosts(P, h->d.bc, h->d.gem_bc, 0, h->st);
-    hook(G_GHOST, 0);
-    hook(G_END, 1);
-    launch_end(P, h->st);
-    hook(G_END, 0);
+  if (!h->prof && nsteps > 1) {  // replay the captured step
+    int rc = capture_step(h);
+    if (rc) return rc;
+    // with a stop time and many steps, look at the stop flag between
+    // chunks instead of queueing steps that would all return at once
+    const bool check = time_stop < 1e299 && nsteps > kStopCheck;
+    for (int n = 0; n < nsteps; n++) {
+      CK(cudaGraphLaunch(h->step_graph, h->st));
+      count_launches(h->step_nodes);
+      if (check && (n + 1) % kStopCheck == 0) {
+        CK(cudaMemcpyAsync(h->hscal, h->scal, NSCAL * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+        if (h->hscal[S_STOP] != 0.0) break;
+      }
+    }
+    CK(cudaGetLastError());
+    return GOP_OK;
   }
+  for (int n = 0; n < nsteps; n++) enqueue_one_step(h, h->st, hook);
   CK(cudaGetLastError());
   return GOP_OK;
 }
@@ -772,6 +827,7 @@ int gop_autotune(gop_instance* h, int reps, int* chosen) {
     }
     h->tune.blk[slot] = cand[best_c];
     if (chosen) chosen[slot] = best_c;
+    drop_step_graph(h);  // the captured step has the old shapes
   }
   cudaEventDestroy(a);
   cudaEventDestroy(b);

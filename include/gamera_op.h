@@ -114,7 +114,10 @@ int gop_prepare(gop_instance *h, int restart);
 
 /* nsteps passes of the time loop (src/solver_solve.c:102-529).  Stops early
  * once time > time_stop (pass a huge value to disable).  Asynchronous with
- * respect to the host unless time_out is non-NULL. */
+ * respect to the host unless time_out is non-NULL, or unless time_stop is
+ * finite and nsteps > 256: the call then looks at the stop flag every 256
+ * steps (synchronising the stream) so it returns soon after time_stop.
+ * More than one step replays a captured CUDA graph of a step. */
 int gop_step(gop_instance *h, int nsteps, double time_stop, double *time_out);
 
 /* Copies the state back in the reference layout: any pointer may be NULL.

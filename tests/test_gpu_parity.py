@@ -101,6 +101,35 @@ def test_orszag_tang_100_steps_matches_oracle(gop, oracle_mod):
     assert st["steps"] == 100
 
 
+def test_orszag_tang_256x256x4_100_steps_matches_reference_binary(gop):
+    """The parity bar at the full Orszag-Tang size: GAMERA-OP's own FP64
+    solver (built from its sources, strict flags, one thread) and the CUDA
+    path start from the reference's step-0 state and must agree to relative
+    L1 <= 1e-10 per variable after 100 steps, with div B at round-off."""
+    ref_run = pytest.importorskip("ref_run")
+    if not ref_run.available("cart", "strict"):
+        pytest.skip("oracle/_ref/ref_cart_strict not built")
+    n = (256, 256, 4)
+    ref = ref_run.run(n, 100, problem="ot", coord="cart",
+                      env={"GOP_BC": "pppppp", "GOP_DOMAIN": "0,1,0,1,0,0.015625"}, timeout=1500)
+    s0, s1 = ref.state(0), ref.state(-1)
+    x = [gop.grid_uniform(n[0], 0.0, 1.0), gop.grid_uniform(n[1], 0.0, 1.0),
+         gop.grid_uniform(n[2], 0.0, 1.0 / 64)]
+    inst = gop.Instance(n, *x)
+    W0 = np.stack([s0[k] for k in ("rho", "v1", "v2", "v3", "p", "pS")])
+    B0 = np.stack([s0[k] for k in ("bi", "bj", "bk")])
+    inst.upload(W0, B0)
+    inst.prepare()
+    inst.step(100)
+    d = inst.download(("gas", "face_b"))
+    Wr = np.stack([s1[k] for k in ("rho", "v1", "v2", "v3", "p", "pS")])
+    Br = np.stack([s1[k] for k in ("bi", "bj", "bk")])
+    compare(n, d["gas"], d["face_b"], Wr, Br, TOL_FP64, "OT 256x256x4 x100 vs reference")
+    st = inst.stats()
+    assert math.isclose(st["time"], s1["time"], rel_tol=1e-12)
+    assert st["divb_max"] < 1e-10
+
+
 def test_blast_3d_matches_oracle(gop, oracle_mod):
     n = (32, 32, 32)
     x = [gop.grid_uniform(m, -0.5, 0.5) for m in n]
