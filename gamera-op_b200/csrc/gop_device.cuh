@@ -178,16 +178,44 @@ __device__ __forceinline__ void load_weights(const R* __restrict__ tab, int tmax
   W.cr2 = __ldg(t0 + (size_t)T_CR2 * tmax);
 }
 
+// Both states of a face (two PDMU7 evaluations).  The two cells adjacent to
+// the face bound both, and the difference across the face that sets the
+// limiter's direction is d1 for the left state and exactly -d1 for the
+// right one, so the clamp bounds, d1 and its sign are computed once; every
+// other operation is the reference's, in its order.
 template <typename R>
 __device__ __forceinline__ void recon_lr(const R v[8], const R lim[4], const FaceWeights<R>& W,
                                          R a1, R a2, R& L, R& Rr) {
-  // left: cells f-4..f+2, limiter cells f-2 (im1), f-1 (i0), f (ip1)
-  L = pdm7<R>(v, W.wl, lim[0], lim[1], lim[2], W.cl1, W.cl2, a1, a2);
-  // right: cells f+3..f-3, limiter f+1 (im1), f (i0), f-1 (ip1)
-  R h[7];
+  const R hi = fmax(lim[1], lim[2]), lo = fmin(lim[1], lim[2]);
+  const R d1 = lim[2] - lim[1];
+  const R s1 = sgn(d1);
+  {
+    // left: cells f-4..f+2, limiter cells f-2 (im1), f-1 (i0), f (ip1)
+    R fi = v[0] * W.wl[0];
 #pragma unroll
-  for (int t = 0; t < 7; t++) h[t] = v[7 - t];
-  Rr = pdm7<R>(h, W.wr, lim[3], lim[2], lim[1], W.cr1, W.cr2, a1, a2);
+    for (int t = 1; t < 7; t++) fi = fma(v[t], W.wl[t], fi);
+    const R f = fmax(lo, fmin(fi, hi));
+    const R d0 = lim[1] - lim[0];
+    const R q0 = fabs(sgn(d0) + s1);
+    const R dl = f - lim[1];
+    R dc = fabs(W.cl1 * lim[1] + W.cl2 * lim[0]) * R(0.5);
+    dc = a1 * dc + a2 * fabs(d0);
+    L = f - s1 * fmax(R(0), fabs(dl) - q0 * dc);
+  }
+  {
+    // right: cells f+3..f-3, limiter cells f+1 (im1), f (i0), f-1 (ip1);
+    // its direction sign is -s1
+    R fi = v[7] * W.wr[0];
+#pragma unroll
+    for (int t = 1; t < 7; t++) fi = fma(v[7 - t], W.wr[t], fi);
+    const R f = fmax(lo, fmin(fi, hi));
+    const R d0 = lim[2] - lim[3];
+    const R q0 = fabs(sgn(d0) - s1);
+    const R dl = f - lim[2];
+    R dc = fabs(W.cr1 * lim[2] + W.cr2 * lim[3]) * R(0.5);
+    dc = a1 * dc + a2 * fabs(d0);
+    Rr = f + s1 * fmax(R(0), fabs(dl) - q0 * dc);
+  }
 }
 
 }  // namespace gop
