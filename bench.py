@@ -51,32 +51,35 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def algorithmic_bytes(group, n):
+def algorithmic_bytes(group, n, mixed=False):
     """Compulsory DRAM bytes of one launch of a kernel group (each input
-    array element read once, each output written once), FP64."""
+    array element read once, each output written once).  Work arrays are
+    FP32 on the mixed path (4 bytes), the state and its AB2 history FP64."""
     ni, nj, nk = n
     cells = ni * nj * nk
     ext = (ni + 9) * (nj + 9) * (nk + 9)
-    if group == "flux":   # per direction: Wh 6, W 6, mags_h 3, mags 3, B_n 1 in; 9 fluxes out
-        return 28 * 8 * (cells + nj * nk)
+    w = 4 if mixed else 8  # element size of the work arrays
+    if group == "flux":   # per direction: Wh 6, W 6, mags_h 3, mags 3, B_n 1 in; 9 fluxes, 2 edge velocities out
+        return 30 * w * (cells + nj * nk)
     if group == "emf":    # per direction: 2 velocities, 2 B_h, 2 B, rho_h in; E out
-        return 8 * 8 * cells
-    if group == "c2c":    # per direction: 2 W_h, 2 W in; 2 edge velocities out
-        return 6 * 8 * (ni + 1) * (nj + 8) * nk
-    if group == "update":  # W 6, B 3, 27 fluxes, 3 EMFs in; W 6, B 3 out
-        return 48 * 8 * cells
-    if group == "ab2":    # W, W_old, B, B_old in; W_h, mags, mags_h, B_h out
-        return 33 * 8 * ext
+        return 8 * w * cells
+    if group == "c2c":    # per direction: 2 W_h, 2 W in; 2 edge velocities out (ghost layers)
+        return 6 * w * (ni + 1) * 8 * nk
+    if group == "update":  # W 6, B 3 in and out (FP64); 27 fluxes, 3 EMFs in
+        return (18 * 8 + 30 * w) * cells
+    if group == "ab2":    # W, W_old, B, B_old in (FP64); W_h, mags, mags_h, B_h out (+ W, B copies when mixed)
+        return (18 * 8 + (15 + (9 if mixed else 0)) * w) * ext
     return 0
 
 
-def ncu_traffic(group):
+def ncu_traffic(group, mixed=False):
     """DRAM bytes per launch from the committed ncu summary, if any."""
     import re
-    f = ROOT / "profiles" / "blast256_kernels.md"
+    f = ROOT / "profiles" / "blast256_launches.md"
     if not f.exists():
         return None
-    m = re.search(rf"^\|\s*{group}\s*\|.*?\|\s*traffic_per_launch_bytes=([\d.e+]+)", f.read_text(), re.M)
+    key = "mixed" if mixed else "fp64"
+    m = re.search(rf"^\|\s*{group}\s*\|.*?\|\s*traffic_per_launch_bytes_{key}=([\d.e+]+)", f.read_text(), re.M)
     return float(m.group(1)) if m else None
 
 
@@ -285,10 +288,10 @@ def main():
     dom = max(groups, key=lambda g: groups[g][0])
     dom_ms, dom_cnt = groups[dom]
     per_launch_s = dom_ms / 1e3 / (dom_cnt * GROUP_LAUNCHES[dom])
-    alg = algorithmic_bytes(dom, n)
+    alg = algorithmic_bytes(dom, n, mixed=prec != 0)
     achieved = alg / per_launch_s / 1e9
     share = {g: round(v[0] / sum(x[0] for x in groups.values()), 4) for g, v in groups.items()}
-    tr = ncu_traffic(dom)
+    tr = ncu_traffic(dom, mixed=prec != 0)
 
     e2e = None
     if not args.no_e2e:
