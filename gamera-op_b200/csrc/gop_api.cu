@@ -94,6 +94,10 @@ double choose(int j, int k) {
   return r;
 }
 
+// stride of the per-axis tables: longest axis + 1, rounded up to a multiple
+// of 4 so the packed face records stay 16-byte aligned
+int table_stride(const int N[3]) { return (std::max(N[0], std::max(N[1], N[2])) + 1 + 3) / 4 * 4; }
+
 struct Tables {
   int tmax;
   std::vector<double> v;
@@ -111,8 +115,8 @@ void build_tables(const gop_desc& d, Tables& T) {
   const double* xs[3] = {d.x1, d.x2, d.x3};
   int N[3];
   for (int a = 0; a < 3; a++) N[a] = n[a] + 2 * NGH + 1;
-  T.tmax = std::max(N[0], std::max(N[1], N[2])) + 1;
-  T.v.assign((size_t)3 * NTAB * T.tmax, 0.0);
+  T.tmax = table_stride(N);
+  T.v.assign(tab_elems(T.tmax), 0.0);
   const bool sph = d.coord == GOP_COORD_SPHERICAL;
   std::vector<double> xctr[3], dxv[3], xcv[3];
   for (int a = 0; a < 3; a++) {
@@ -255,6 +259,20 @@ void build_tables(const gop_desc& d, Tables& T) {
         T.at(a, T_WL0 + t, f) = wl[t];
         T.at(a, T_WR0 + t, f) = wr[t];
       }
+    }
+  }
+  // the same weights and coefficients packed per face (see FW)
+  for (int a = 0; a < 3; a++) {
+    for (int f = 0; f < T.tmax; f++) {
+      double* r = T.v.data() + fw_offset(T.tmax) + ((size_t)a * T.tmax + f) * FW;
+      for (int t = 0; t < 7; t++) {
+        r[t] = T.at(a, T_WL0 + t, f);
+        r[7 + t] = T.at(a, T_WR0 + t, f);
+      }
+      r[14] = T.at(a, T_CL1, f);
+      r[15] = T.at(a, T_CL2, f);
+      r[16] = T.at(a, T_CR1, f);
+      r[17] = T.at(a, T_CR2, f);
     }
   }
 }
@@ -402,10 +420,10 @@ size_t gop_footprint(const gop_desc* d) {
   Layout L = layout_of(d);
   size_t rsize = d->precision == GOP_PREC_MIXED ? sizeof(float) : sizeof(double);
   size_t ref = (size_t)L.N[0] * L.N[1] * L.N[2];
-  size_t tmax = std::max(L.N[0], std::max(L.N[1], L.N[2])) + 1;
+  const size_t tab = tab_elems(table_stride(L.N));
   const bool mixed = d->precision == GOP_PREC_MIXED;
   return (size_t)L.fs * (18 * sizeof(double) + work_fields(mixed) * rsize) +
-         6 * ref * sizeof(double) + 3 * NTAB * tmax * (sizeof(double) + (mixed ? sizeof(float) : 0)) +
+         6 * ref * sizeof(double) + tab * (sizeof(double) + (mixed ? sizeof(float) : 0)) +
          NSCAL * sizeof(double);
 }
 
@@ -510,11 +528,13 @@ int gop_create(const gop_desc* desc, gop_instance** out) {
   if (d.precision == GOP_PREC_MIXED) {
     float* w = (float*)h->work;
     h->wf = Work<float>{w, w + 6 * L.fs, w + 9 * L.fs, w + 12 * L.fs, w + 15 * L.fs,
-                        w + 21 * L.fs, w + 24 * L.fs, w + 51 * L.fs, w + 57 * L.fs, h->tabf};
+                        w + 21 * L.fs, w + 24 * L.fs, w + 51 * L.fs, w + 57 * L.fs, h->tabf,
+                        h->tabf + fw_offset(T.tmax)};
   } else {
     double* w = (double*)h->work;
     h->wd = Work<double>{w, w + 6 * L.fs, w + 9 * L.fs, w + 12 * L.fs, w + 15 * L.fs,
-                         w + 21 * L.fs, w + 24 * L.fs, nullptr, nullptr, h->tab};
+                         w + 21 * L.fs, w + 24 * L.fs, nullptr, nullptr, h->tab,
+                         h->tab + fw_offset(T.tmax)};
   }
   cudaError_t le = cudaStreamSynchronize(h->st);
   if (le == cudaSuccess) le = cudaGetLastError();

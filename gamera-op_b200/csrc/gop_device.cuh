@@ -42,6 +42,15 @@ enum Tab : int {
   NTAB
 };
 
+// The PDM weights and limiter coefficients of one face packed together
+// after the per-axis tables: fw[(axis * tmax + f) * FW + t], t = 0..6 left
+// weights, 7..13 right weights, 14..17 cl1 cl2 cr1 cr2, 18..19 zero, so one
+// face's 18 values come in five 16-byte loads (FP32) from one address.
+// tmax is a multiple of 4, which keeps every face record 16-byte aligned.
+constexpr int FW = 20;
+__host__ __device__ constexpr size_t fw_offset(int tmax) { return (size_t)3 * NTAB * tmax; }
+__host__ __device__ constexpr size_t tab_elems(int tmax) { return (size_t)3 * (NTAB + FW) * tmax; }
+
 // device scalars (one double slot each)
 enum Scal : int {
   S_DT = 0,      // dt of the current step
@@ -178,29 +187,60 @@ __device__ __forceinline__ void load_weights(const R* __restrict__ tab, int tmax
   W.cr2 = __ldg(t0 + (size_t)T_CR2 * tmax);
 }
 
-// Both states of a face (two PDMU7 evaluations).  The two cells adjacent to
-// the face bound both, and the difference across the face that sets the
-// limiter's direction is d1 for the left state and exactly -d1 for the
-// right one, so the clamp bounds, d1 and its sign are computed once; every
-// other operation is the reference's, in its order.
+// the same from the packed face records (fw = the packed region): one
+// address and five (FP32) or nine (FP64) vector loads per face
+__device__ __forceinline__ void load_fw(const float* __restrict__ fw, int tmax, int axis, int f,
+                                        FaceWeights<float>& W) {
+  const float4* p = reinterpret_cast<const float4*>(fw + ((size_t)axis * tmax + f) * FW);
+  const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3), e = __ldg(p + 4);
+  W.wl[0] = a.x; W.wl[1] = a.y; W.wl[2] = a.z; W.wl[3] = a.w;
+  W.wl[4] = b.x; W.wl[5] = b.y; W.wl[6] = b.z; W.wr[0] = b.w;
+  W.wr[1] = c.x; W.wr[2] = c.y; W.wr[3] = c.z; W.wr[4] = c.w;
+  W.wr[5] = d.x; W.wr[6] = d.y; W.cl1 = d.z; W.cl2 = d.w;
+  W.cr1 = e.x; W.cr2 = e.y;
+}
+__device__ __forceinline__ void load_fw(const double* __restrict__ fw, int tmax, int axis, int f,
+                                        FaceWeights<double>& W) {
+  const double2* p = reinterpret_cast<const double2*>(fw + ((size_t)axis * tmax + f) * FW);
+  double v[18];
+#pragma unroll
+  for (int t = 0; t < 9; t++) {
+    const double2 q = __ldg(p + t);
+    v[2 * t] = q.x;
+    v[2 * t + 1] = q.y;
+  }
+#pragma unroll
+  for (int t = 0; t < 7; t++) {
+    W.wl[t] = v[t];
+    W.wr[t] = v[7 + t];
+  }
+  W.cl1 = v[14]; W.cl2 = v[15]; W.cr1 = v[16]; W.cr2 = v[17];
+}
+
+// Both states of a face (two PDMU7 evaluations) from the half-step line
+// v[0..7] = cells f-4..f+3 and the step-start values lim[0..3] = cells
+// f-2..f+1.  With D(g) = lim(g) - lim(g-1) the limiter of the left state
+// needs sgn D(f-1), |D(f-1)| and sgn D(f); the right one (its differences
+// taken in the mirrored direction, lim(f) - lim(f+1) = -D(f+1) exactly)
+// needs sgn D(f+1), |D(f+1)| and sgn D(f), so the caller passes
+// s1 = sgn D(f), q0l = |sgn D(f-1) + s1| and q0r = |sgn D(f+1) + s1|.
+// a1h = a1/2: the reference's |c1 p0 + c2 pm1| * 0.5 * a1 with the exact
+// factor 1/2 moved into a1.  Every other operation is the reference's, in
+// its order.
 template <typename R>
-__device__ __forceinline__ void recon_lr(const R v[8], const R lim[4], const FaceWeights<R>& W,
-                                         R a1, R a2, R& L, R& Rr) {
+__device__ __forceinline__ void pdm_pair(const R v[8], const R lim[4], const FaceWeights<R>& W,
+                                         R a1h, R a2, R s1, R q0l, R q0r, R L_ad0, R R_ad0,
+                                         R& L, R& Rr) {
   const R hi = fmax(lim[1], lim[2]), lo = fmin(lim[1], lim[2]);
-  const R d1 = lim[2] - lim[1];
-  const R s1 = sgn(d1);
   {
     // left: cells f-4..f+2, limiter cells f-2 (im1), f-1 (i0), f (ip1)
     R fi = v[0] * W.wl[0];
 #pragma unroll
     for (int t = 1; t < 7; t++) fi = fma(v[t], W.wl[t], fi);
     const R f = fmax(lo, fmin(fi, hi));
-    const R d0 = lim[1] - lim[0];
-    const R q0 = fabs(sgn(d0) + s1);
     const R dl = f - lim[1];
-    R dc = fabs(W.cl1 * lim[1] + W.cl2 * lim[0]) * R(0.5);
-    dc = a1 * dc + a2 * fabs(d0);
-    L = f - s1 * fmax(R(0), fabs(dl) - q0 * dc);
+    const R dc = a1h * fabs(W.cl1 * lim[1] + W.cl2 * lim[0]) + a2 * L_ad0;
+    L = f - s1 * fmax(R(0), fabs(dl) - q0l * dc);
   }
   {
     // right: cells f+3..f-3, limiter cells f+1 (im1), f (i0), f-1 (ip1);
@@ -209,13 +249,30 @@ __device__ __forceinline__ void recon_lr(const R v[8], const R lim[4], const Fac
 #pragma unroll
     for (int t = 1; t < 7; t++) fi = fma(v[7 - t], W.wr[t], fi);
     const R f = fmax(lo, fmin(fi, hi));
-    const R d0 = lim[2] - lim[3];
-    const R q0 = fabs(sgn(d0) - s1);
     const R dl = f - lim[2];
-    R dc = fabs(W.cr1 * lim[2] + W.cr2 * lim[3]) * R(0.5);
-    dc = a1 * dc + a2 * fabs(d0);
-    Rr = f + s1 * fmax(R(0), fabs(dl) - q0 * dc);
+    const R dc = a1h * fabs(W.cr1 * lim[2] + W.cr2 * lim[3]) + a2 * R_ad0;
+    Rr = f + s1 * fmax(R(0), fabs(dl) - q0r * dc);
   }
+}
+
+// one face on its own: the three differences of lim computed here
+template <typename R>
+__device__ __forceinline__ void recon_lr(const R v[8], const R lim[4], const FaceWeights<R>& W,
+                                         R a1h, R a2, R& L, R& Rr) {
+  const R dm = lim[1] - lim[0], d1 = lim[2] - lim[1], dp = lim[3] - lim[2];
+  const R s1 = sgn(d1);
+  pdm_pair<R>(v, lim, W, a1h, a2, s1, fabs(sgn(dm) + s1), fabs(sgn(dp) + s1), fabs(dm),
+              fabs(dp), L, Rr);
+}
+
+// Weights of face f on axis AX for a warp whose lanes run along i: along
+// i every lane has its own face, and the tap-major tables give coalesced
+// loads; along j or k the whole warp shares one face record.
+template <int AX, typename R>
+__device__ __forceinline__ void load_face_weights(const R* __restrict__ tab, const R* __restrict__ fw,
+                                                  int tmax, int f, FaceWeights<R>& W) {
+  if constexpr (AX == 0) load_weights<R>(tab, tmax, 0, f, W);
+  else load_fw(fw, tmax, AX, f, W);
 }
 
 }  // namespace gop

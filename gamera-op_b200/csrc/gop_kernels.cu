@@ -256,8 +256,8 @@ __device__ __forceinline__ void c2c_body(const Params& P, const Work<R>& wk, Pos
   const size_t fs = P.fs;
   const R* __restrict__ W = lim_w<R>(P, wk) + x;
   FaceWeights<R> Wt;
-  load_weights<R>(wk.tab, P.tmax, p, f, Wt);
-  const R a1 = (R)P.pdm_a1, a2 = (R)P.pdm_a2;
+  load_face_weights<p, R>(wk.tab, wk.fw, P.tmax, f, Wt);
+  const R a1h = (R)(0.5 * P.pdm_a1), a2 = (R)P.pdm_a2;
 #pragma unroll
   for (int cc = 0; cc < 2; cc++) {
     const int comp = cc == 0 ? p : q;
@@ -265,7 +265,7 @@ __device__ __forceinline__ void c2c_body(const Params& P, const Work<R>& wk, Pos
     line8<R, R>(wk.Wh + (size_t)(V1 + comp) * fs + x, s, v);
 #pragma unroll
     for (int u = 0; u < 4; u++) lim[u] = W[(V1 + comp) * fs + (u - 2) * s];
-    recon_lr<R>(v, lim, Wt, a1, a2, L, Rr);
+    recon_lr<R>(v, lim, Wt, a1h, a2, L, Rr);
     wk.V[x + (size_t)(2 * D + cc) * fs] = R(0.5) * (L + Rr);
   }
 }
@@ -286,18 +286,18 @@ __device__ __forceinline__ void emf_body(const Params& P, const Work<R>& wk, Pos
   const long long x = lin(P, i, j, k), sp = sd<p>(P), sq = sd<q>(P);
   const size_t fs = P.fs;
   const R* __restrict__ B = lim_b<R>(P, wk) + x;
-  const R a1 = (R)P.pdm_a1, a2 = (R)P.pdm_a2;
+  const R a1h = (R)(0.5 * P.pdm_a1), a2 = (R)P.pdm_a2;
   R vav[2], bpl, bpr, bql, bqr;
   {
     FaceWeights<R> Wt;
-    load_weights<R>(wk.tab, P.tmax, q, pos[q], Wt);
+    load_face_weights<q, R>(wk.tab, wk.fw, P.tmax, pos[q], Wt);
 #pragma unroll
     for (int cc = 0; cc < 2; cc++) {
       R v[8], lim[4], L, Rr;
       line8<R, R>(wk.V + (size_t)(2 * D + cc) * fs + x, sq, v);
 #pragma unroll
       for (int u = 0; u < 4; u++) lim[u] = v[u + 2];
-      recon_lr<R>(v, lim, Wt, a1, a2, L, Rr);
+      recon_lr<R>(v, lim, Wt, a1h, a2, L, Rr);
       vav[cc] = R(0.5) * (L + Rr);
     }
     // B_p along q
@@ -305,17 +305,17 @@ __device__ __forceinline__ void emf_body(const Params& P, const Work<R>& wk, Pos
     line8<R, R>(wk.Bh + (size_t)p * fs + x, sq, v);
 #pragma unroll
     for (int u = 0; u < 4; u++) lim[u] = B[p * fs + (u - 2) * sq];
-    recon_lr<R>(v, lim, Wt, a1, a2, bpl, bpr);
+    recon_lr<R>(v, lim, Wt, a1h, a2, bpl, bpr);
   }
   {
     // B_q along p
     FaceWeights<R> Wt;
-    load_weights<R>(wk.tab, P.tmax, p, pos[p], Wt);
+    load_face_weights<p, R>(wk.tab, wk.fw, P.tmax, pos[p], Wt);
     R v[8], lim[4];
     line8<R, R>(wk.Bh + (size_t)q * fs + x, sp, v);
 #pragma unroll
     for (int u = 0; u < 4; u++) lim[u] = B[q * fs + (u - 2) * sp];
-    recon_lr<R>(v, lim, Wt, a1, a2, bql, bqr);
+    recon_lr<R>(v, lim, Wt, a1h, a2, bql, bqr);
   }
   const R bp = R(0.5) * (bpl + bpr), bq = R(0.5) * (bql + bqr);
   const R vp = vav[0], vq = vav[1];
@@ -333,40 +333,15 @@ __device__ __forceinline__ void emf_body(const Params& P, const Work<R>& wk, Pos
 
 // ------------------------------------------------------------ face flux
 
-// Rusanov hydro flux and Maxwell stress at faces normal to D
-// (src/solver_func.c:934-1529).  F[9] = mass, 3 momenta, energy, entropy,
-// 3 stress components.
+// Rusanov hydro flux and Maxwell stress at the face normal to D at cell x
+// from the reconstructed states (src/solver_func.c:934-1529).  F[9] =
+// mass, 3 momenta, energy, entropy, 3 stress components.  Also writes the
+// first centre-to-edge sweep of edges along (D+2)%3 (see c2c_body).
 template <typename R, int D>
-__device__ __forceinline__ void flux_body(const Params& P, const Work<R>& wk, Pos t) {
-  const int i = NGH + t.x, j = NGH + t.y, k = NGH + t.z;
-  if (i >= NGH + P.n[0] + (D == 0) || j >= NGH + P.n[1] + (D == 1) ||
-      k >= NGH + P.n[2] + (D == 2))
-    return;
-  const int f = D == 0 ? i : (D == 1 ? j : k);
-  const long long x = lin(P, i, j, k), s = sd<D>(P);
+__device__ __forceinline__ void flux_out(const Params& P, const Work<R>& wk, long long x,
+                                         const R L[6], const R Rt[6], const R mL[3],
+                                         const R mR[3]) {
   const size_t fs = P.fs;
-  const R* __restrict__ W = lim_w<R>(P, wk) + x;
-  FaceWeights<R> Wt;
-  load_weights<R>(wk.tab, P.tmax, D, f, Wt);
-  const R a1 = (R)P.pdm_a1, a2 = (R)P.pdm_a2;
-  R L[6], Rt[6], mL[3], mR[3];
-#pragma unroll
-  for (int m = 0; m < 6; m++) {
-    R v[8], lim[4];
-    line8<R, R>(wk.Wh + (size_t)m * fs + x, s, v);
-#pragma unroll
-    for (int u = 0; u < 4; u++) lim[u] = W[m * fs + (u - 2) * s];
-    recon_lr<R>(v, lim, Wt, a1, a2, L[m], Rt[m]);
-  }
-#pragma unroll
-  for (int a = 0; a < 3; a++) {
-    R v[8], lim[4];
-    line8<R, R>(wk.Msh + (size_t)a * fs + x, s, v);
-    const R* ms = wk.Ms + (size_t)a * fs + x;
-#pragma unroll
-    for (int u = 0; u < 4; u++) lim[u] = ms[(u - 2) * s];
-    recon_lr<R>(v, lim, Wt, a1, a2, mL[a], mR[a]);
-  }
   const R gm = (R)P.gamma, gm1 = (R)P.gm1, ca = (R)P.ca, ca2 = (R)P.ca2;
   const R rl = L[RHO], rr = Rt[RHO], pl = L[PR], pr = Rt[PR], sl = L[PS], sr = Rt[PS];
   const R irl = R(1) / rl, irr = R(1) / rr;
@@ -433,6 +408,41 @@ __device__ __forceinline__ void flux_body(const Params& P, const Work<R>& wk, Po
     }
     o[(6 + a) * fs] = (tl + tr) - bq * (Rt[V1 + a] - L[V1 + a]);
   }
+}
+
+// PDM reconstruction of the 9 face states, then flux_out: one thread per face
+template <typename R, int D>
+__device__ __forceinline__ void flux_body(const Params& P, const Work<R>& wk, Pos t) {
+  const int i = NGH + t.x, j = NGH + t.y, k = NGH + t.z;
+  if (i >= NGH + P.n[0] + (D == 0) || j >= NGH + P.n[1] + (D == 1) ||
+      k >= NGH + P.n[2] + (D == 2))
+    return;
+  const int f = D == 0 ? i : (D == 1 ? j : k);
+  const long long x = lin(P, i, j, k), s = sd<D>(P);
+  const size_t fs = P.fs;
+  const R* __restrict__ W = lim_w<R>(P, wk) + x;
+  FaceWeights<R> Wt;
+  load_face_weights<D, R>(wk.tab, wk.fw, P.tmax, f, Wt);
+  const R a1h = (R)(0.5 * P.pdm_a1), a2 = (R)P.pdm_a2;
+  R L[6], Rt[6], mL[3], mR[3];
+#pragma unroll
+  for (int m = 0; m < 6; m++) {
+    R v[8], lim[4];
+    line8<R, R>(wk.Wh + (size_t)m * fs + x, s, v);
+#pragma unroll
+    for (int u = 0; u < 4; u++) lim[u] = W[m * fs + (u - 2) * s];
+    recon_lr<R>(v, lim, Wt, a1h, a2, L[m], Rt[m]);
+  }
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    R v[8], lim[4];
+    line8<R, R>(wk.Msh + (size_t)a * fs + x, s, v);
+    const R* ms = wk.Ms + (size_t)a * fs + x;
+#pragma unroll
+    for (int u = 0; u < 4; u++) lim[u] = ms[(u - 2) * s];
+    recon_lr<R>(v, lim, Wt, a1h, a2, mL[a], mR[a]);
+  }
+  flux_out<R, D>(P, wk, x, L, Rt, mL, mR);
 }
 
 // --------------------------------------------------------------- update

@@ -21,6 +21,7 @@ struct Work {
   R* Wl;   // FP32 path: 6 step-start primitives in R (the limiters' reference)
   R* Bl;   // FP32 path: 3 step-start face fields in R
   const R* tab;  // the per-axis tables in R (same layout as Params::tab)
+  const R* fw;   // the packed face records in R (tab + fw_offset(tmax))
 };
 constexpr int WORK_FIELDS = 6 + 3 + 3 + 3 + 6 + 3 + 27;
 // the FP32 path adds the R copies of the step-start state (Wl, Bl)
