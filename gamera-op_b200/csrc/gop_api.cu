@@ -951,7 +951,7 @@ static int batch_slot_used(const gop_instance* h, int slot) {
 
 static dim3 batch_block(const gop_batch* b, int slot) {
   if (slot == K_UPDATE_SPH) return b->tune.blk[K_UPDATE];
-  return slot < NTUNE ? b->tune.blk[slot] : dim3(32, 8, 1);
+  return slot < NTUNE ? b->tune.blk[slot] : ghost_block(slot);
 }
 
 // work items of one side and slot with block shape blk; false if a grid

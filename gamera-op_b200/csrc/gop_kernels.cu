@@ -802,16 +802,17 @@ __device__ __forceinline__ void dt_body(const Params& P, Pos t, double& dtc, dou
 // Space: (N[oa], N[ob], 2*NGH); sources (active layers) and destinations
 // (ghost layers) are disjoint for n >= NGH, so both sides go in one launch.
 __device__ __forceinline__ void wrap_body(const Params& P, int axis, int which, Pos t) {
-  const int oa = (axis + 1) % 3, ob = (axis + 2) % 3;
-  if (t.x >= P.N[oa] || t.y >= P.N[ob] || t.z >= 2 * NGH) return;
+  // t = (i, j, k) with the component along `axis` replaced by the ghost
+  // layer 0..2*NGH-1, so lanes run along i (along the layers for axis 0)
+  int ijk[3] = {t.x, t.y, t.z};
+  const int lay = ijk[axis];
+  for (int a = 0; a < 3; a++)
+    if (ijk[a] >= (a == axis ? 2 * NGH : P.N[a])) return;
   const int bsel = which ? cur_buf(P) : 1 - cur_buf(P);
   double* __restrict__ W = P.Wbuf[bsel];
   double* __restrict__ B = P.Bbuf[bsel];
   const int N = P.N[axis];
-  const int side = t.z / NGH, l = t.z % NGH;
-  int ijk[3];
-  ijk[oa] = t.x;
-  ijk[ob] = t.y;
+  const int side = lay / NGH, l = lay % NGH;
   for (int f = 0; f < 9; f++) {
     const int onface = (f >= 6 && f - 6 == axis) ? 1 : 0;
     double* a = f < 6 ? W + (size_t)f * P.fs : B + (size_t)(f - 6) * P.fs;
@@ -832,18 +833,18 @@ __device__ __forceinline__ void wrap_body(const Params& P, int axis, int which, 
 
 // One face of the ghost-fill library (src/boundary_conditions.c): the 6 gas
 // primitives with kind `kind` (gas_bc_*) and the 3 face fields with kind
-// `gkind` (gem_bc_*); 0 skips that group.  Space: (N[oa], N[ob], NGH).
+// `gkind` (gem_bc_*); 0 skips that group.  t = (i, j, k) with the
+// component along `axis` replaced by the ghost layer 0..NGH-1.
 __device__ __forceinline__ void bcface_body(const Params& P, int axis, int side, int kind,
                                             int gkind, int which, Pos t) {
-  const int oa = (axis + 1) % 3, ob = (axis + 2) % 3;
-  if (t.x >= P.N[oa] || t.y >= P.N[ob] || t.z >= NGH) return;
+  int ijk[3] = {t.x, t.y, t.z};
+  const int l = ijk[axis];
+  for (int a = 0; a < 3; a++)
+    if (ijk[a] >= (a == axis ? NGH : P.N[a])) return;
   const int bsel = which ? cur_buf(P) : 1 - cur_buf(P);
   double* __restrict__ W = P.Wbuf[bsel];
   double* __restrict__ B = P.Bbuf[bsel];
-  const int N = P.N[axis], l = t.z;
-  int ijk[3];
-  ijk[oa] = t.x;
-  ijk[ob] = t.y;
+  const int N = P.N[axis];
   for (int f = 0; f < 9; f++) {
     const bool gas = f < 6;
     const int kd = gas ? kind : gkind;
@@ -1121,13 +1122,12 @@ Tune::Tune() {
 dim3 launch_space(const Params& P, int slot) {
   if (slot == K_AB2) return dim3(P.N[0], P.N[1], P.N[2]);
   if (slot == K_UPDATE || slot == K_UPDATE_SPH) return dim3(P.n[0], P.n[1], P.n[2]);
-  if (slot >= K_WRAP0 && slot <= K_WRAP2) {
-    const int a = slot - K_WRAP0;
-    return dim3(P.N[(a + 1) % 3], P.N[(a + 2) % 3], 2 * NGH);
-  }
-  if (slot >= K_BC0 && slot <= K_BC5) {
-    const int a = (slot - K_BC0) / 2;
-    return dim3(P.N[(a + 1) % 3], P.N[(a + 2) % 3], NGH);
+  if (slot >= K_WRAP0 && slot <= K_BC5) {  // (i, j, k) with the ghost layers along the axis
+    const bool wrap = slot <= K_WRAP2;
+    const int a = wrap ? slot - K_WRAP0 : (slot - K_BC0) / 2;
+    int e[3] = {P.N[0], P.N[1], P.N[2]};
+    e[a] = wrap ? 2 * NGH : NGH;
+    return dim3(e[0], e[1], e[2]);
   }
   const int stage = (slot - K_C2C0) / 3, D = (slot - K_C2C0) % 3;
   const int p = (D + 1) % 3, q = (D + 2) % 3;
@@ -1215,14 +1215,19 @@ template void launch_step_body<double>(const Params&, int, const Work<double>&, 
 template void launch_step_body<float>(const Params&, int, const Work<float>&, cudaStream_t,
                                       const Tune&, const Hook&);
 
+dim3 ghost_block(int slot) {
+  if (slot == K_WRAP0) return dim3(8, 16, 2);               // 8 layers along i
+  if (slot == K_BC0 || slot == K_BC1) return dim3(4, 32, 2);  // 4 layers along i
+  return dim3(32, 8, 1);
+}
+
 void launch_ghosts(const Params& P, const char bc[6], const char gem_bc[6], int which,
                    cudaStream_t st) {
-  const dim3 blk(32, 8, 1);
   bool periodic[3];
   for (int a = 0; a < 3; a++) periodic[a] = bc[2 * a] == 'p' && bc[2 * a + 1] == 'p';
   for (int a = 0; a < 3; a++) {
     if (!periodic[a]) continue;
-    const dim3 sp = launch_space(P, K_WRAP0 + a);
+    const dim3 sp = launch_space(P, K_WRAP0 + a), blk = ghost_block(K_WRAP0 + a);
     LAUNCH(k_wrap, grid3(sp.x, sp.y, sp.z, blk), blk, st, P, a, which);
   }
   for (int face = 0; face < 6; face++) {
@@ -1232,7 +1237,7 @@ void launch_ghosts(const Params& P, const char bc[6], const char gem_bc[6], int 
     const bool gas_work = kind != 'n';
     const bool gem_work = gkind != 'n' && gkind != 'r';
     if (!gas_work && !gem_work) continue;
-    const dim3 sp = launch_space(P, K_BC0 + face);
+    const dim3 sp = launch_space(P, K_BC0 + face), blk = ghost_block(K_BC0 + face);
     LAUNCH(k_bcface, grid3(sp.x, sp.y, sp.z, blk), blk, st, P, a, side, (int)kind, (int)gkind, which);
   }
 }

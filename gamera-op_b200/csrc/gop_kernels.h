@@ -49,6 +49,8 @@ struct Tune {
 
 // points covered by the launch of one slot (x, y, z extents)
 dim3 launch_space(const Params& P, int slot);
+// thread-block shape of a ghost-fill slot (K_WRAP*, K_BC*)
+dim3 ghost_block(int slot);
 
 // one member of a batch: its parameters, work arrays and boundary kinds
 template <typename R>
