@@ -344,8 +344,8 @@ def _accuracy(gop, n, got, want):
 
 def bench_batched(args, gop, torch, dist, rank, world, local, max_all, barrier):
     """96 independent OT / blast grids of uneven size advanced in one batch
-    (mixed precision, autotuned block shapes) against the same grids run one
-    at a time on the plain FP64 path (gop_step per grid)."""
+    (mixed precision) against the same grids run one at a time on the plain
+    FP64 path (gop_step per grid); both with autotuned block shapes."""
     from collections import Counter
     from gop import serve, workloads
     jobs = workloads.batched_uneven(count=args.members, steps=args.steps)
@@ -379,6 +379,9 @@ def bench_batched(args, gop, torch, dist, rank, world, local, max_all, barrier):
 
     def serial(prec):
         insts = [workloads.build(j, precision=prec) for j in mine]
+        tb = gop.Batch(insts)  # only to give them the same per-class tuning
+        tb.autotune(reps=2)
+        tb.close()
         for i in insts:
             i.set_stream(stream.cuda_stream)
             i.step(W, sync=False)

@@ -906,163 +906,72 @@ int gop_get_stats(gop_instance* h, gop_stats* out) {
 
 }  // extern "C"
 
-// A batch advances many independent grids with one launch per stage: the
-// blocks of every member's launch of a stage are concatenated into one work
-// list, so small grids that could not fill the GPU alone fill it together.
-// Each member keeps its own device scalars (dt, time, AB2 coefficient, step
-// budget); one captured batched step is replayed max(steps) times and a
-// member whose budget is spent skips the rest.
-struct BatchSide {
-  int n = 0;
-  void* members = nullptr;  // device Member<R>[n]
-  BatchLists L{};
-  int* steps = nullptr;     // device int[n]
-};
+// A batch advances many independent grids as one CUDA graph per step.  The
+// graph holds every member's own step -- its single-instance launch
+// sequence, with its parameters as kernel arguments -- on up to kBranches
+// parallel branches (members placed largest first on the branch with the
+// fewest cells so far), so small grids that could not fill the GPU alone
+// run side by side, and the launches of one grid's memory-bound stages
+// overlap other grids' compute-bound ones.  Each member keeps its own
+// device scalars (dt, time, AB2 coefficient, step budget); the graph is
+// replayed max(steps) times and a member whose budget is spent returns at
+// once from every launch.
+static const int kBranches = 16;
 
 struct gop_batch {
   std::vector<gop_instance*> m;
-  std::vector<int> idx[2];  // member indices per precision (0: FP64, 1: mixed)
-  BatchSide side[2];
-  Tune tune;                // block shapes of the tunable slots
-  void* dev = nullptr;      // one device allocation for members, lists and steps
-  int* hsteps = nullptr;    // host staging of the step budgets
-  int64_t nodes = 0;        // kernels in one replay of the graph
+  int64_t nodes = 0;           // kernels in one replay of the graph
   cudaStream_t own = nullptr;  // capture stream
   cudaStream_t st = nullptr;   // launch stream (own, or the caller's)
+  std::vector<cudaStream_t> br;  // branch streams (used while capturing)
+  std::vector<cudaEvent_t> ev;   // fork and join events of the capture
   cudaGraphExec_t graph = nullptr;
 };
 
-static int batch_slot_used(const gop_instance* h, int slot) {
-  const char* bc = h->d.bc;
-  const char* gbc = h->d.gem_bc;
-  if (slot == K_UPDATE) return h->d.coord == GOP_COORD_CARTESIAN;
-  if (slot == K_UPDATE_SPH) return h->d.coord != GOP_COORD_CARTESIAN;
-  if (slot < NTUNE) return 1;
-  if (slot <= K_WRAP2) {
-    const int a = slot - K_WRAP0;
-    return bc[2 * a] == 'p' && bc[2 * a + 1] == 'p';
-  }
-  const int face = slot - K_BC0, a = face / 2;
-  if (bc[2 * a] == 'p' && bc[2 * a + 1] == 'p') return 0;
-  const bool gas_work = bc[face] != 'n';
-  const bool gem_work = gbc[face] != 'n' && gbc[face] != 'r';
-  return gas_work || gem_work;
-}
-
-static dim3 batch_block(const gop_batch* b, int slot) {
-  if (slot == K_UPDATE_SPH) return b->tune.blk[K_UPDATE];
-  return slot < NTUNE ? b->tune.blk[slot] : ghost_block(slot);
-}
-
-// work items of one side and slot with block shape blk; false if a grid
-// needs more than 65535 blocks along an axis
-static bool batch_items(const gop_batch* b, int s, int slot, dim3 blk,
-                        std::vector<unsigned long long>& out) {
-  out.clear();
-  for (int li = 0; li < (int)b->idx[s].size(); li++) {
-    const gop_instance* h = b->m[b->idx[s][li]];
-    if (!batch_slot_used(h, slot)) continue;
-    const dim3 sp = launch_space(h->P, slot);
-    const unsigned gx = (sp.x + blk.x - 1) / blk.x, gy = (sp.y + blk.y - 1) / blk.y,
-                   gz = (sp.z + blk.z - 1) / blk.z;
-    if (gx > 0xffff || gy > 0xffff || gz > 0xffff) return false;
-    for (unsigned z = 0; z < gz; z++)
-      for (unsigned y = 0; y < gy; y++)
-        for (unsigned x = 0; x < gx; x++)
-          out.push_back(((unsigned long long)li << 48) | ((unsigned long long)x << 32) |
-                        ((unsigned long long)y << 16) | z);
-  }
-  return true;
-}
-
 static void batch_release(gop_batch* b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
-  if (b->dev) cudaFreeAsync(b->dev, b->own);
   b->graph = nullptr;
-  b->dev = nullptr;
 }
 
-// (re)builds the device images of the members and work lists with the
-// batch's block shapes, and captures one batched step
+// captures one step of every member into the batch graph
 static int batch_build(gop_batch* b) {
   batch_release(b);
-  std::vector<unsigned long long> items[2][NSLOT];
-  std::vector<Member<double>> md;
-  std::vector<Member<float>> mf;
-  for (int s = 0; s < 2; s++) {
-    for (int li = 0; li < (int)b->idx[s].size(); li++) {
-      gop_instance* h = b->m[b->idx[s][li]];
-      if (s == 0) {
-        Member<double> M{};
-        M.P = h->P;
-        M.w = h->wd;
-        for (int f = 0; f < 6; f++) M.bc[f] = h->d.bc[f], M.gbc[f] = h->d.gem_bc[f];
-        md.push_back(M);
-      } else {
-        Member<float> M{};
-        M.P = h->P;
-        M.w = h->wf;
-        for (int f = 0; f < 6; f++) M.bc[f] = h->d.bc[f], M.gbc[f] = h->d.gem_bc[f];
-        mf.push_back(M);
-      }
-    }
-    for (int slot = 0; slot < NSLOT; slot++)
-      if (!batch_items(b, s, slot, batch_block(b, slot), items[s][slot]))
-        return fail(GOP_EINVAL, "a member is too large for a batch");
-  }
-  size_t off = 0;
-  auto place = [&](size_t bytes) {
-    size_t o = (off + 255) & ~(size_t)255;
-    off = o + bytes;
-    return o;
+  const int nb = (int)b->br.size();
+  std::vector<int> order(b->m.size());
+  for (size_t i = 0; i < order.size(); i++) order[i] = (int)i;
+  auto cells = [&](int i) {
+    const gop_desc& d = b->m[i]->d;
+    return (long long)d.ni * d.nj * d.nk;
   };
-  size_t o_mem[2], o_items[2][NSLOT], o_steps[2];
-  o_mem[0] = place(md.size() * sizeof(Member<double>));
-  o_mem[1] = place(mf.size() * sizeof(Member<float>));
-  for (int s = 0; s < 2; s++) {
-    for (int slot = 0; slot < NSLOT; slot++) o_items[s][slot] = place(items[s][slot].size() * 8);
-    o_steps[s] = place(b->idx[s].size() * sizeof(int));
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cells(x) > cells(y); });
+  std::vector<long long> load(nb, 0);
+  std::vector<int> branch(b->m.size(), 0);
+  for (int i : order) {
+    const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    branch[i] = k;
+    load[k] += cells(i);
   }
-  cudaError_t e = cudaMallocAsync(&b->dev, off, b->own);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(b->own);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    b->dev = nullptr;
-    return fail(GOP_ENOMEM, "batch allocation of %zu bytes failed: %s", off, cudaGetErrorString(e));
-  }
-  char* base = (char*)b->dev;
-  CK(cudaMemcpyAsync(base + o_mem[0], md.data(), md.size() * sizeof(Member<double>),
-                     cudaMemcpyHostToDevice, b->own));
-  CK(cudaMemcpyAsync(base + o_mem[1], mf.data(), mf.size() * sizeof(Member<float>),
-                     cudaMemcpyHostToDevice, b->own));
-  for (int s = 0; s < 2; s++) {
-    BatchSide& S = b->side[s];
-    S.n = (int)b->idx[s].size();
-    S.members = base + o_mem[s];
-    S.steps = (int*)(base + o_steps[s]);
-    for (int slot = 0; slot < NSLOT; slot++) {
-      CK(cudaMemcpyAsync(base + o_items[s][slot], items[s][slot].data(), items[s][slot].size() * 8,
-                         cudaMemcpyHostToDevice, b->own));
-      S.L.count[slot] = (int)items[s][slot].size();
-      S.L.blk[slot] = batch_block(b, slot);
-      S.L.items[slot] = (const unsigned long long*)(base + o_items[s][slot]);
-    }
-  }
-  CK(cudaStreamSynchronize(b->own));  // the host images above go out of scope
+  CK(cudaStreamSynchronize(b->own));
   cudaGraph_t g = nullptr;
   const int64_t before = launches();
   CK(cudaStreamBeginCapture(b->own, cudaStreamCaptureModeThreadLocal));
-  if (b->side[0].n)
-    launch_batch_step<double>((const Member<double>*)b->side[0].members, b->side[0].n, b->side[0].L, b->own);
-  if (b->side[1].n)
-    launch_batch_step<float>((const Member<float>*)b->side[1].members, b->side[1].n, b->side[1].L, b->own);
-  e = cudaStreamEndCapture(b->own, &g);
+  cudaError_t e = cudaEventRecord(b->ev[0], b->own);
+  for (int k = 0; k < nb && e == cudaSuccess; k++) e = cudaStreamWaitEvent(b->br[k], b->ev[0], 0);
+  if (e == cudaSuccess)
+    for (int i : order) enqueue_one_step(b->m[i], b->br[branch[i]], Hook());
+  for (int k = 0; k < nb && e == cudaSuccess; k++) {
+    e = cudaEventRecord(b->ev[1 + k], b->br[k]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->own, b->ev[1 + k], 0);
+  }
+  cudaError_t e2 = cudaStreamEndCapture(b->own, &g);
+  if (e == cudaSuccess) e = e2;
   // captured launches run at each replay, not now
   b->nodes = launches() - before;
   count_launches(-b->nodes);
   if (e == cudaSuccess) e = cudaGraphInstantiate(&b->graph, g, 0);
   if (g) cudaGraphDestroy(g);
   if (e != cudaSuccess) {
+    cudaGetLastError();
     b->graph = nullptr;
     return fail(GOP_ECUDA, "batch graph capture failed: %s", cudaGetErrorString(e));
   }
@@ -1084,11 +993,17 @@ int gop_batch_create(gop_instance* const* members, int count, gop_batch** out) {
   gop_batch* b = new (std::nothrow) gop_batch();
   if (!b) return fail(GOP_ENOMEM, "host allocation failed");
   b->m.assign(members, members + count);
-  for (int i = 0; i < count; i++) b->idx[members[i]->d.precision == GOP_PREC_MIXED ? 1 : 0].push_back(i);
+  const int nb = std::min(count, kBranches);
   cudaError_t e = cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking);
-  if (e == cudaSuccess) {
-    b->hsteps = new (std::nothrow) int[count];
-    if (!b->hsteps) e = cudaErrorMemoryAllocation;
+  for (int k = 0; k < nb && e == cudaSuccess; k++) {
+    cudaStream_t s = nullptr;
+    e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) b->br.push_back(s);
+  }
+  for (int k = 0; k <= nb && e == cudaSuccess; k++) {
+    cudaEvent_t ev = nullptr;
+    e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) b->ev.push_back(ev);
   }
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -1109,7 +1024,8 @@ int gop_batch_destroy(gop_batch* b) {
   if (!b) return GOP_OK;
   if (b->st) cudaStreamSynchronize(b->st);
   batch_release(b);
-  delete[] b->hsteps;
+  for (cudaStream_t s : b->br) cudaStreamDestroy(s);
+  for (cudaEvent_t ev : b->ev) cudaEventDestroy(ev);
   if (b->own) cudaStreamDestroy(b->own);
   delete b;
   return GOP_OK;
@@ -1122,105 +1038,39 @@ int gop_batch_set_stream(gop_batch* b, void* stream) {
   return GOP_OK;
 }
 
-// Batch autotuner: for each tunable slot, times every candidate block shape
-// on the batched launch of that slot over all members and keeps the
-// fastest, then rebuilds the work lists.  The members must be freshly
-// prepared (no restart, no step yet): the history buffers then equal the
-// state, so the update launches' writes into them are undone by copying the
-// state over them again.
+// Batch autotuner: members of the same grid shape, geometry and precision
+// share block shapes; gop_autotune chooses them on the first member of each
+// such class (restoring its state afterwards), the others copy them, and the
+// batch graph is captured again.  `chosen` receives the choice of the class
+// with the most cells.
 int gop_batch_autotune(gop_batch* b, int reps, int* chosen) {
   if (!b) return fail(GOP_EINVAL, "batch is NULL");
-  if (reps <= 0) reps = 3;
-  for (size_t i = 0; i < b->m.size(); i++)
-    if (!b->m[i]->fresh) return fail(GOP_ESTATE, "member %zu is not freshly prepared", i);
   CK(cudaStreamSynchronize(b->st));
-  std::vector<std::vector<double>> saved(b->m.size());
+  std::vector<int> rep(b->m.size(), -1);
+  long long most = -1;
   for (size_t i = 0; i < b->m.size(); i++) {
-    gop_instance* h = b->m[i];
-    CK(cudaMemcpyAsync(h->hscal, h->scal, NSCAL * sizeof(double), cudaMemcpyDeviceToHost, h->st));
-    CK(cudaStreamSynchronize(h->st));
-    saved[i].assign(h->hscal, h->hscal + NSCAL);
-    if (saved[i][S_PAR] != 0.0) return fail(GOP_ESTATE, "member %zu is not freshly prepared", i);
-  }
-  const int ncand = kNumBlockCandidates;
-  // largest list over candidates and slots, per side
-  size_t most = 0;
-  std::vector<unsigned long long> items;
-  for (int s = 0; s < 2; s++)
-    for (int slot = 0; slot < NSLOT; slot++)
-      for (int c = 0; c < ncand; c++) {
-        if (!batch_items(b, s, slot, kBlockCandidates[c], items)) continue;
-        most = std::max(most, items.size());
-      }
-  unsigned long long* ditems = nullptr;
-  CK(cudaMallocAsync((void**)&ditems, std::max<size_t>(most, 1) * 8, b->own));
-  CK(cudaStreamSynchronize(b->own));
-  cudaEvent_t ea, eb;
-  CK(cudaEventCreate(&ea));
-  CK(cudaEventCreate(&eb));
-  int rc = GOP_OK;
-  for (int slot = 0; slot < NTUNE && rc == GOP_OK; slot++) {
-    float best = 1e30f;
-    int best_c = -1;
-    for (int c = 0; c < ncand; c++) {
-      const dim3 blk = kBlockCandidates[c];
-      float total = 0.f;
-      bool ok = true;
-      for (int part = 0; part < 2 * (slot == K_UPDATE ? 2 : 1) && ok; part++) {
-        const int s = part % 2;
-        const int sl = part >= 2 ? K_UPDATE_SPH : slot;  // the update has two lists
-        if (!b->side[s].n) continue;
-        if (!batch_items(b, s, sl, blk, items)) {
-          ok = false;
-          break;
-        }
-        if (cudaMemcpyAsync(ditems, items.data(), items.size() * 8, cudaMemcpyHostToDevice,
-                            b->own) != cudaSuccess) {
-          rc = fail(GOP_ECUDA, "autotune upload failed");
-          ok = false;
-          break;
-        }
-        for (int r = 0; r <= reps; r++) {
-          if (r == 1) cudaEventRecord(ea, b->own);
-          if (s == 0)
-            launch_batch_slot<double>((const Member<double>*)b->side[0].members, sl, (int)items.size(), blk, ditems, b->own);
-          else
-            launch_batch_slot<float>((const Member<float>*)b->side[1].members, sl, (int)items.size(), blk, ditems, b->own);
-        }
-        cudaEventRecord(eb, b->own);
-        if (cudaEventSynchronize(eb) != cudaSuccess) {
-          rc = fail(GOP_ECUDA, "autotune launch failed: %s", cudaGetErrorString(cudaGetLastError()));
-          ok = false;
-          break;
-        }
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, ea, eb);
-        total += ms;
-      }
-      if (ok && total < best) {
-        best = total;
-        best_c = c;
-      }
+    const gop_desc& d = b->m[i]->d;
+    for (size_t k = 0; k < i && rep[i] < 0; k++) {
+      const gop_desc& e = b->m[k]->d;
+      if (d.ni == e.ni && d.nj == e.nj && d.nk == e.nk && d.coord == e.coord &&
+          d.precision == e.precision)
+        rep[i] = rep[k];
     }
-    if (best_c >= 0) b->tune.blk[slot] = kBlockCandidates[best_c];
-    if (chosen) chosen[slot] = best_c;
+    if (rep[i] >= 0) {
+      b->m[i]->tune = b->m[rep[i]]->tune;
+      drop_step_graph(b->m[i]);
+      continue;
+    }
+    rep[i] = (int)i;
+    int pick[NTUNE];
+    const int rc = gop_autotune(b->m[i], reps, pick);
+    if (rc) return rc;
+    const long long cells = (long long)d.ni * d.nj * d.nk;
+    if (chosen && cells > most) {
+      most = cells;
+      for (int t = 0; t < NTUNE; t++) chosen[t] = pick[t];
+    }
   }
-  cudaEventDestroy(ea);
-  cudaEventDestroy(eb);
-  cudaFreeAsync(ditems, b->own);
-  // undo the update launches: history <- state, scalars as they were
-  for (size_t i = 0; i < b->m.size(); i++) {
-    gop_instance* h = b->m[i];
-    const Params& P = h->P;
-    CK(cudaMemcpyAsync(P.Wbuf[1], P.Wbuf[0], (size_t)P.fs * 6 * sizeof(double),
-                       cudaMemcpyDeviceToDevice, b->own));
-    CK(cudaMemcpyAsync(P.Bbuf[1], P.Bbuf[0], (size_t)P.fs * 3 * sizeof(double),
-                       cudaMemcpyDeviceToDevice, b->own));
-    for (int t = 0; t < NSCAL; t++) h->hscal[t] = saved[i][t];
-    CK(cudaMemcpyAsync(h->scal, h->hscal, NSCAL * sizeof(double), cudaMemcpyHostToDevice, b->own));
-    CK(cudaStreamSynchronize(b->own));
-  }
-  if (rc) return rc;
   return batch_build(b);
 }
 
@@ -1234,15 +1084,7 @@ int gop_batch_launch(gop_batch* b, const int* steps) {
   // members' own streams may still hold work on their state
   for (gop_instance* h : b->m) CK(cudaStreamSynchronize(h->st));
   CK(cudaStreamSynchronize(b->st));  // the previous launch of this batch is done
-  for (int s = 0; s < 2; s++) {
-    BatchSide& S = b->side[s];
-    if (!S.n) continue;
-    int* hs = b->hsteps + (s == 0 ? 0 : b->side[0].n);
-    for (int li = 0; li < S.n; li++) hs[li] = steps[b->idx[s][li]];
-    CK(cudaMemcpyAsync(S.steps, hs, S.n * sizeof(int), cudaMemcpyHostToDevice, b->st));
-    if (s == 0) launch_batch_arm<double>((const Member<double>*)S.members, S.n, S.steps, b->st);
-    else launch_batch_arm<float>((const Member<float>*)S.members, S.n, S.steps, b->st);
-  }
+  for (size_t i = 0; i < b->m.size(); i++) launch_arm(b->m[i]->P, 1e300, (double)steps[i], b->st);
   for (int n = 0; n < most; n++) CK(cudaGraphLaunch(b->graph, b->st));
   count_launches((int64_t)most * b->nodes);
   for (size_t i = 0; i < b->m.size(); i++)

@@ -15,10 +15,9 @@
 //   ghost     periodic wrap and boundary fills of the new state
 //   end       the written buffer becomes the current state
 //
-// Every stage is a per-point body function used by two kernel forms: a
-// single-instance kernel (the launch grid covers one grid) and a batched
-// kernel whose blocks come from a work list of (instance, block) items, so
-// one launch advances every member of a batch of uneven grids.
+// Every stage is a per-point body function of a kernel whose launch grid
+// covers one grid; a batch of grids captures each member's launches on
+// parallel branches of one CUDA graph.
 //
 // R is the arithmetic type of the reconstruction / flux / EMF stages
 // (double: plain path; float: mixed path).  The state, the AB2
@@ -144,14 +143,6 @@ __device__ __forceinline__ Pos grid_pos() {
   return {(int)(blockIdx.x * blockDim.x + threadIdx.x), (int)(blockIdx.y * blockDim.y + threadIdx.y),
           (int)(blockIdx.z * blockDim.z + threadIdx.z)};
 }
-// batched launches: item = (member << 48) | (bx << 32) | (by << 16) | bz
-__device__ __forceinline__ Pos item_pos(unsigned long long it, int& member) {
-  member = (int)(it >> 48);
-  const int bx = (int)((it >> 32) & 0xffff), by = (int)((it >> 16) & 0xffff), bz = (int)(it & 0xffff);
-  return {(int)(bx * blockDim.x + threadIdx.x), (int)(by * blockDim.y + threadIdx.y),
-          (int)(bz * blockDim.z + threadIdx.z)};
-}
-
 // ---------------------------------------------------------- step control
 
 // open the step (src/solver_solve.c:103-107, src/solver_func.c:385-491):
@@ -964,94 +955,6 @@ __global__ void k_bcface(Params P, int axis, int side, int kind, int gkind, int 
   bcface_body(P, axis, side, kind, gkind, which, grid_pos());
 }
 
-// -------------------------------------------------------- batched kernels
-// Each block handles one (member, block) item of a work list built on the
-// host; members are independent grids with their own scalars.
-
-template <typename R>
-__global__ void kb_begin(const Member<R>* __restrict__ m, int n) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n) begin_body(m[t].P);
-}
-template <typename R>
-__global__ void kb_end(const Member<R>* __restrict__ m, int n) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n) end_body(m[t].P);
-}
-template <typename R>
-__global__ void kb_arm(const Member<R>* __restrict__ m, int n, const int* __restrict__ steps) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n) arm_body(m[t].P, 1e300, (double)steps[t]);
-}
-
-template <typename R>
-__global__ void __launch_bounds__(256, GOP_MINB(AB2, R)) kb_ab2(const Member<R>* __restrict__ m,
-                                              const unsigned long long* __restrict__ items) {
-  int mi;
-  const Pos t = item_pos(items[blockIdx.x], mi);
-  const Member<R>& M = m[mi];
-  if (stopped(M.P)) return;
-  ab2_body<R>(M.P, M.w, t);
-}
-template <typename R, int D>
-__global__ void __launch_bounds__(256, GOP_MINB(C2C, R)) kb_c2c(const Member<R>* __restrict__ m,
-                                              const unsigned long long* __restrict__ items) {
-  int mi;
-  const Pos t = item_pos(items[blockIdx.x], mi);
-  const Member<R>& M = m[mi];
-  if (stopped(M.P)) return;
-  c2c_body<R, D>(M.P, M.w, t);
-}
-template <typename R, int D>
-__global__ void __launch_bounds__(256, GOP_MINB(EMF, R)) kb_emf(const Member<R>* __restrict__ m,
-                                              const unsigned long long* __restrict__ items) {
-  int mi;
-  const Pos t = item_pos(items[blockIdx.x], mi);
-  const Member<R>& M = m[mi];
-  if (stopped(M.P)) return;
-  emf_body<R, D>(M.P, M.w, t);
-}
-template <typename R, int D>
-__global__ void __launch_bounds__(256, GOP_MINB(FLUX, R)) kb_flux(const Member<R>* __restrict__ m,
-                                                  const unsigned long long* __restrict__ items) {
-  int mi;
-  const Pos t = item_pos(items[blockIdx.x], mi);
-  const Member<R>& M = m[mi];
-  if (stopped(M.P)) return;
-  flux_body<R, D>(M.P, M.w, t);
-}
-// Cartesian and spherical members have separate work lists (K_UPDATE,
-// K_UPDATE_SPH) so each kernel is compiled for one geometry
-template <int COORD, typename R>
-__global__ void __launch_bounds__(256, GOP_UPD_MINB(COORD, R)) kb_update(const Member<R>* __restrict__ m,
-                                                    const unsigned long long* __restrict__ items) {
-  int mi;
-  const Pos t = item_pos(items[blockIdx.x], mi);
-  const Member<R>& M = m[mi];
-  if (stopped(M.P)) return;  // block-uniform: the whole block returns
-  double dtc = DBL_MAX, db = 0.0;
-  update_body<COORD, R>(M.P, M.w, t, dtc, db);
-  block_commit(dtc, db, M.P.scal + S_NEXT_DT, M.P.scal + S_DIVB);
-}
-template <typename R>
-__global__ void kb_wrap(const Member<R>* __restrict__ m, const unsigned long long* __restrict__ items,
-                        int axis) {
-  int mi;
-  const Pos t = item_pos(items[blockIdx.x], mi);
-  const Member<R>& M = m[mi];
-  if (stopped(M.P)) return;
-  wrap_body(M.P, axis, 0, t);
-}
-template <typename R>
-__global__ void kb_bcface(const Member<R>* __restrict__ m, const unsigned long long* __restrict__ items,
-                          int face) {
-  int mi;
-  const Pos t = item_pos(items[blockIdx.x], mi);
-  const Member<R>& M = m[mi];
-  if (stopped(M.P)) return;
-  bcface_body(M.P, face / 2, face % 2, M.bc[face], M.gbc[face], 0, t);
-}
-
 // ------------------------------------------------------ layout transposes
 
 // reference layout [f][i][j][k] (k fastest) <-> device layout
@@ -1121,7 +1024,7 @@ Tune::Tune() {
 
 dim3 launch_space(const Params& P, int slot) {
   if (slot == K_AB2) return dim3(P.N[0], P.N[1], P.N[2]);
-  if (slot == K_UPDATE || slot == K_UPDATE_SPH) return dim3(P.n[0], P.n[1], P.n[2]);
+  if (slot == K_UPDATE) return dim3(P.n[0], P.n[1], P.n[2]);
   if (slot >= K_WRAP0 && slot <= K_BC5) {  // (i, j, k) with the ghost layers along the axis
     const bool wrap = slot <= K_WRAP2;
     const int a = wrap ? slot - K_WRAP0 : (slot - K_BC0) / 2;
@@ -1241,61 +1144,6 @@ void launch_ghosts(const Params& P, const char bc[6], const char gem_bc[6], int 
     LAUNCH(k_bcface, grid3(sp.x, sp.y, sp.z, blk), blk, st, P, a, side, (int)kind, (int)gkind, which);
   }
 }
-
-// batched step: one launch per stage over the work lists of all members
-template <typename R>
-void launch_batch_arm(const Member<R>* m, int n, const int* steps, cudaStream_t st) {
-  LAUNCH(kb_arm<R>, (n + 127) / 128, 128, st, m, n, steps);
-}
-template void launch_batch_arm<double>(const Member<double>*, int, const int*, cudaStream_t);
-template void launch_batch_arm<float>(const Member<float>*, int, const int*, cudaStream_t);
-
-template <typename R>
-void launch_batch_slot(const Member<R>* m, int slot, int count, dim3 blk,
-                       const unsigned long long* items, cudaStream_t st) {
-  if (count <= 0) return;
-  switch (slot) {
-    case K_AB2: LAUNCH(kb_ab2<R>, count, blk, st, m, items); break;
-    case K_C2C0: LAUNCH((kb_c2c<R, 0>), count, blk, st, m, items); break;
-    case K_C2C1: LAUNCH((kb_c2c<R, 1>), count, blk, st, m, items); break;
-    case K_C2C2: LAUNCH((kb_c2c<R, 2>), count, blk, st, m, items); break;
-    case K_EMF0: LAUNCH((kb_emf<R, 0>), count, blk, st, m, items); break;
-    case K_EMF1: LAUNCH((kb_emf<R, 1>), count, blk, st, m, items); break;
-    case K_EMF2: LAUNCH((kb_emf<R, 2>), count, blk, st, m, items); break;
-    case K_FLUX0: LAUNCH((kb_flux<R, 0>), count, blk, st, m, items); break;
-    case K_FLUX1: LAUNCH((kb_flux<R, 1>), count, blk, st, m, items); break;
-    case K_FLUX2: LAUNCH((kb_flux<R, 2>), count, blk, st, m, items); break;
-    case K_UPDATE: LAUNCH((kb_update<0, R>), count, blk, st, m, items); break;
-    case K_UPDATE_SPH: LAUNCH((kb_update<2, R>), count, blk, st, m, items); break;
-    case K_WRAP0: case K_WRAP1: case K_WRAP2:
-      LAUNCH(kb_wrap<R>, count, blk, st, m, items, slot - K_WRAP0);
-      break;
-    default:
-      if (slot >= K_BC0 && slot <= K_BC5) LAUNCH(kb_bcface<R>, count, blk, st, m, items, slot - K_BC0);
-      break;
-  }
-}
-template void launch_batch_slot<double>(const Member<double>*, int, int, dim3, const unsigned long long*, cudaStream_t);
-template void launch_batch_slot<float>(const Member<float>*, int, int, dim3, const unsigned long long*, cudaStream_t);
-
-template <typename R>
-void launch_batch_step(const Member<R>* m, int n, const BatchLists& L, cudaStream_t st) {
-  const int nb = (n + 127) / 128;
-  LAUNCH(kb_begin<R>, nb, 128, st, m, n);
-  // the stages in step order (flux before the first edge sweep, which it
-  // partly computes); the ghost fill after both updates
-  static const int order[] = {K_AB2, K_FLUX0, K_FLUX1, K_FLUX2, K_C2C0, K_C2C1, K_C2C2,
-                              K_EMF0, K_EMF1, K_EMF2, K_UPDATE};
-  for (int slot : order)
-    launch_batch_slot<R>(m, slot, L.count[slot], L.blk[slot], L.items[slot], st);
-  launch_batch_slot<R>(m, K_UPDATE_SPH, L.count[K_UPDATE_SPH], L.blk[K_UPDATE_SPH],
-                       L.items[K_UPDATE_SPH], st);
-  for (int slot = K_WRAP0; slot <= K_BC5; slot++)
-    launch_batch_slot<R>(m, slot, L.count[slot], L.blk[slot], L.items[slot], st);
-  LAUNCH(kb_end<R>, nb, 128, st, m, n);
-}
-template void launch_batch_step<double>(const Member<double>*, int, const BatchLists&, cudaStream_t);
-template void launch_batch_step<float>(const Member<float>*, int, const BatchLists&, cudaStream_t);
 
 void launch_from_ref(const Params& P, int nf, const double* src, double* dst, cudaStream_t st) {
   const dim3 blk(32, 8, 1);

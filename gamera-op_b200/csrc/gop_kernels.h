@@ -33,15 +33,13 @@ void count_launches(int64_t n);  // kernels run by graph replays
 // kernel groups of one step, for event timing
 enum Group : int { G_BEGIN = 0, G_AB2, G_C2C, G_EMF, G_FLUX, G_UPDATE, G_GHOST, G_END, NGROUP };
 
-// launch shapes of the tunable kernels: AB2, C2C x3, EMF x3, FLUX x3, UPDATE;
-// then the slots of the batched work lists only: the ghost launches
-// (periodic wrap per axis, boundary fill per face) and the update of
-// spherical members (K_UPDATE then holds the Cartesian ones; both use the
-// UPDATE block shape)
+// launch shapes of the tunable kernels: AB2, C2C x3, EMF x3, FLUX x3,
+// UPDATE; then the ghost launches (periodic wrap per axis, boundary fill
+// per face), whose shapes are fixed (ghost_block)
 enum TuneSlot : int { K_AB2 = 0, K_C2C0, K_C2C1, K_C2C2, K_EMF0, K_EMF1, K_EMF2,
                       K_FLUX0, K_FLUX1, K_FLUX2, K_UPDATE, NTUNE,
                       K_WRAP0 = NTUNE, K_WRAP1, K_WRAP2, K_BC0, K_BC1, K_BC2, K_BC3, K_BC4,
-                      K_BC5, K_UPDATE_SPH, NSLOT };
+                      K_BC5, NSLOT };
 struct Tune {
   dim3 blk[NTUNE];
   Tune();
@@ -51,23 +49,6 @@ struct Tune {
 dim3 launch_space(const Params& P, int slot);
 // thread-block shape of a ghost-fill slot (K_WRAP*, K_BC*)
 dim3 ghost_block(int slot);
-
-// one member of a batch: its parameters, work arrays and boundary kinds
-template <typename R>
-struct Member {
-  Params P;
-  Work<R> w;
-  int bc[6];   // gas kind per face ('p','s','r','f','e','n'); wrap done by K_WRAP*
-  int gbc[6];  // face-field kind per face
-};
-
-// per-slot work lists of a batch: items[slot][b] = (member << 48) |
-// (block x << 32) | (block y << 16) | block z, blocks of shape blk[slot]
-struct BatchLists {
-  int count[NSLOT];
-  dim3 blk[NSLOT];
-  const unsigned long long* items[NSLOT];  // device arrays
-};
 
 // launches one tunable kernel alone (for the autotuner)
 template <typename R>
@@ -93,16 +74,6 @@ void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t
 // which = 0: the buffer being written this step; 1: the current state
 void launch_ghosts(const Params& P, const char bc[6], const char gem_bc[6], int which,
                    cudaStream_t st);
-// batched step of n members (device array m): every stage one launch over
-// the work lists; members whose budget is spent skip the step
-template <typename R>
-void launch_batch_arm(const Member<R>* m, int n, const int* steps, cudaStream_t st);
-template <typename R>
-void launch_batch_step(const Member<R>* m, int n, const BatchLists& L, cudaStream_t st);
-// one slot's batched launch alone (for the batch autotuner)
-template <typename R>
-void launch_batch_slot(const Member<R>* m, int slot, int count, dim3 blk,
-                       const unsigned long long* items, cudaStream_t st);
 void launch_from_ref(const Params& P, int nf, const double* src, double* dst, cudaStream_t st);
 void launch_to_ref(const Params& P, int nf, const double* src, double* dst, cudaStream_t st);
 template <typename R>

@@ -4,7 +4,8 @@ Requests arrive over time (``Job.arrival``, seconds from the start).  The
 loop admits them in arrival order while a slot is free and their device
 footprint fits an HBM budget, keeps every admitted grid resident on the GPU,
 and advances all live grids together in rounds of at most ``chunk`` steps
-(one batched launch per stage over all live grids).  A request leaves as
+(one CUDA graph per step holding every live grid's launches on parallel
+branches).  A request leaves as
 soon as its own steps are done: its result is copied back, its memory is
 freed and the next waiting request takes the slot.  Requests that arrive
 while a round runs are set up on the host and device during the round and

@@ -215,12 +215,14 @@ int gop_problem_init(const gop_desc *desc, const gop_problem *p, double *gas, do
 typedef struct gop_batch gop_batch;
 
 /* Groups instances (all already prepared, each at most once, at most 65535)
- * so one call advances each by its own number of steps.  Every stage of a
- * step is one launch over the blocks of all members (a work list of
- * (member, block) items built here), captured once in a CUDA graph; the
- * members may differ in size, geometry, boundary kinds and precision.  The
- * members must outlive the batch.  No counterpart in the reference, which
- * runs one domain per process. */
+ * so one call advances each by its own number of steps.  One step of all
+ * members is captured once in a CUDA graph: each member's own launch
+ * sequence (its gop_step launches) on one of up to 16 parallel branches,
+ * largest members placed first on the least-loaded branch, so the members
+ * run side by side; the graph is replayed max(steps) times.  The members
+ * may differ in size, geometry, boundary kinds and precision.  The members
+ * must outlive the batch.  No counterpart in the reference, which runs one
+ * domain per process. */
 int gop_batch_create(gop_instance *const *members, int count, gop_batch **out);
 int gop_batch_destroy(gop_batch *b);
 /* steps[m] >= 0 per member (indexed as at creation); returns when all are
@@ -238,12 +240,12 @@ int gop_batch_wait(gop_batch *b);
 /* Launches of the batch go to `stream` (cudaStream_t as void*; NULL: the
  * batch's own non-blocking stream). */
 int gop_batch_set_stream(gop_batch *b, void *stream);
-/* Times every candidate thread-block shape (the gop_autotune list) on the
- * batched launch of each tunable kernel over all members, keeps the
- * fastest and rebuilds the work lists; chosen[GOP_NTUNE] (may be NULL)
- * receives the candidate index per kernel.  All members must be freshly
- * prepared (gop_prepare without restart, no step since): the state and
- * scalars are left as they were.  GOP_ESTATE otherwise. */
+/* Chooses thread-block shapes for the members: gop_autotune on the first
+ * member of each class of equal grid shape, geometry and precision, copied
+ * to the rest of the class, then captures the batch graph again;
+ * chosen[GOP_NTUNE] (may be NULL) receives the candidate indices of the
+ * class with the most cells.  The state and scalars of every member are
+ * left as they were. */
 int gop_batch_autotune(gop_batch *b, int reps, int *chosen);
 
 #ifdef __cplusplus
