@@ -141,29 +141,6 @@ __device__ __forceinline__ R sgn(R x) {
   return x > R(0) ? R(1) : (x < R(0) ? R(-1) : R(0));
 }
 
-// PDMU7 (src/solver_func.c:215-253): 7-tap interpolation of the half-step
-// values h[0..6], clamped to the two step-start values adjacent to the face,
-// then the PDM limiter with the geometric reference slope
-// |c1*p0 + c2*pm1|/2 blended with |p0 - pm1|.
-template <typename R>
-__device__ __forceinline__ R pdm7(const R h[7], const R w[7], R pm1, R p0, R pp1, R c1, R c2,
-                                  R a1, R a2) {
-  R fi = h[0] * w[0];
-#pragma unroll
-  for (int t = 1; t < 7; t++) fi = fma(h[t], w[t], fi);
-  R hi = fmax(p0, pp1);
-  R lo = fmin(p0, pp1);
-  R f = fmax(lo, fmin(fi, hi));
-  R d0 = p0 - pm1;
-  R d1 = pp1 - p0;
-  R s1 = sgn(d1);
-  R q0 = fabs(sgn(d0) + s1);
-  R dl = f - p0;
-  R dc = fabs(c1 * p0 + c2 * pm1) * R(0.5);
-  dc = a1 * dc + a2 * fabs(d0);
-  return f - s1 * fmax(R(0), fabs(dl) - q0 * dc);
-}
-
 // Left and right states at face f of a line v[0..7] = cells f-4..f+3, with
 // the limiter on lim[0..3] = cells f-2..f+1.
 template <typename R>
@@ -217,7 +194,11 @@ __device__ __forceinline__ void load_fw(const double* __restrict__ fw, int tmax,
   W.cl1 = v[14]; W.cl2 = v[15]; W.cr1 = v[16]; W.cr2 = v[17];
 }
 
-// Both states of a face (two PDMU7 evaluations) from the half-step line
+// Both states of a face (two evaluations of PDMU7, src/solver_func.c:215-253:
+// a 7-tap interpolation of the half-step values, clamped to the two
+// step-start values adjacent to the face, then the PDM limiter with the
+// geometric reference slope |c1*p0 + c2*pm1|/2 blended with |p0 - pm1|)
+// from the half-step line
 // v[0..7] = cells f-4..f+3 and the step-start values lim[0..3] = cells
 // f-2..f+1.  With D(g) = lim(g) - lim(g-1) the limiter of the left state
 // needs sgn D(f-1), |D(f-1)| and sgn D(f); the right one (its differences
