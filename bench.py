@@ -451,12 +451,12 @@ def bench_served(args, gop, torch, dist, rank, world, local, max_all, barrier):
     launches = gop.kernel_launches() - launches0
     eng.close()
     served = serve.combine(rep, dist)
-    pool, init = {}, {}
+    pool = {}
     kept = {o.rid: o.result for o in rep.outcomes if o.rid % 8 == 0}
     worst, divb = (0.0, ""), 0.0
 
     def run_one(j):
-        inst = workloads.build(j, precision=gop.PREC_FP64, host=init)
+        inst = workloads.build(j, precision=gop.PREC_FP64, device_init=True)
         inst.step(j.steps)
         res = serve.download_result(inst, pool, copy=j.rid in kept)
         inst.close()

@@ -16,10 +16,12 @@ SOURCES = [
     PKG / "csrc" / "gop_api.cu",
     PKG / "csrc" / "gop_kernels.cu",
     PKG / "csrc" / "gop_noalloc.cu",
+    PKG / "csrc" / "gop_init.cu",
     PKG / "host" / "gop_problems.c",
 ]
 HEADERS = [ROOT / "include" / "gamera_op.h", PKG / "csrc" / "gop_device.cuh",
-           PKG / "csrc" / "gop_kernels.h", PKG / "csrc" / "gop_internal.h"]
+           PKG / "csrc" / "gop_kernels.h", PKG / "csrc" / "gop_internal.h",
+           PKG / "csrc" / "gop_fields.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -598,6 +598,38 @@ int gop_upload(gop_instance* h, const double* gas, const double* face_b, const d
   return GOP_OK;
 }
 
+int gop_problem_init_device(gop_instance* h, const gop_problem* p) {
+  if (!h || !p) return fail(GOP_EINVAL, "NULL argument");
+  const bool sph = h->d.coord == GOP_COORD_SPHERICAL;
+  switch (p->kind) {
+    case GOP_PROBLEM_OT:
+    case GOP_PROBLEM_BLAST:
+    case GOP_PROBLEM_LOOP_CART:
+      if (sph) return fail(GOP_EINVAL, "problem %d needs a Cartesian grid", p->kind);
+      break;
+    case GOP_PROBLEM_LOOP_SPH:
+      if (!sph) return fail(GOP_EINVAL, "problem %d needs a spherical grid", p->kind);
+      break;
+    default:
+      return fail(GOP_EINVAL, "unknown problem kind %d", p->kind);
+  }
+  const Params& P = h->P;
+  // the state goes to buffer 0 (as gop_upload puts it), zero where the
+  // problem leaves it; the work arrays (>= 3 fields of doubles) are free
+  // until gop_prepare and hold the edge integrals
+  CK(cudaMemsetAsync(P.Wbuf[0], 0, (size_t)P.fs * 6 * sizeof(double), h->st));
+  CK(cudaMemsetAsync(P.Bbuf[0], 0, (size_t)P.fs * 3 * sizeof(double), h->st));
+  launch_problem_init(P, *p, sph ? 1 : 0, (double*)h->work, h->st);
+  CK(cudaGetLastError());
+  double* s = h->hscal;
+  CK(cudaStreamSynchronize(h->st));
+  for (int t = 0; t < NSCAL; t++) s[t] = 0.0;
+  CK(cudaMemcpyAsync(h->scal, s, NSCAL * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  h->prepared = false;
+  return GOP_OK;
+}
+
 int gop_prepare(gop_instance* h, int restart) {
   if (!h) return fail(GOP_EINVAL, "instance is NULL");
   const Params& P = h->P;

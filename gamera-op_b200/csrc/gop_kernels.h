@@ -4,6 +4,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "gamera_op.h"
 #include "gop_device.cuh"
 
 namespace gop {
@@ -79,5 +80,9 @@ void launch_to_ref(const Params& P, int nf, const double* src, double* dst, cuda
 template <typename R>
 void launch_widen(const Params& P, int nf, const R* src, double* dst, cudaStream_t st);
 void launch_mags(const Params& P, const double* B, double* out, cudaStream_t st);
+// problem p's initial state in buffer 0 (cells, face field; ghosts left for
+// the ghost fill); scratch: 3 fields of doubles for the edge integrals
+void launch_problem_init(const Params& P, const gop_problem& p, int sph, double* scratch,
+                         cudaStream_t st);
 
 }  // namespace gop

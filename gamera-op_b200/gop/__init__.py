@@ -90,6 +90,7 @@ def lib():
         L.gop_grid_uniform.argtypes = [C.c_int, C.c_double, C.c_double, _dp]
         L.gop_problem_defaults.argtypes = [C.c_int, C.POINTER(Problem)]
         L.gop_problem_init.argtypes = [C.POINTER(Desc), C.POINTER(Problem), _dp, _dp]
+        L.gop_problem_init_device.argtypes = [vp, C.POINTER(Problem)]
         L.gop_autotune.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
         L.gop_set_profiling.argtypes = [vp, C.c_int]
         L.gop_get_profile.argtypes = [vp, _dp, C.POINTER(C.c_int64)]
@@ -208,6 +209,12 @@ class Instance:
         p = problem(kind, **over)
         _check(lib().gop_problem_init(C.byref(self.desc), C.byref(p), _ptr(gas), _ptr(fb)))
         return gas, fb
+
+    def init_problem_device(self, kind: int, **over):
+        """Builds a problem's initial state on the device, in place of
+        init_problem + upload (gop_problem_init_device); prepare follows."""
+        p = problem(kind, **over)
+        _check(lib().gop_problem_init_device(self._h, C.byref(p)))
 
     def upload(self, gas, face_b, gas_p=None, face_b_p=None, time=0.0, dt0=0.0):
         gas = _contig(gas, self.shape(6))

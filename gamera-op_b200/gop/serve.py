@@ -15,7 +15,7 @@ The loop is written against a small engine interface so its scheduling can
 be tested on the CPU with a fake engine:
 
 * ``footprint(job) -> int`` device bytes of the job's state
-* ``create(job) -> handle`` allocate, initialise and prepare
+* ``create(job) -> handle`` allocate, initialise (on the GPU) and prepare
 * ``launch(handles, steps)`` / ``wait()`` advance live grids by per-grid steps
 * ``finish(job, handle) -> result`` copy the result back and free the grid
 
@@ -219,11 +219,12 @@ class GpuEngine:
     gop.Batch over the live set (built for the next round while the current
     one runs)."""
 
-    def __init__(self, keep=lambda job: False, precision=None):
+    def __init__(self, keep=lambda job: False, precision=None, device_init=True):
         from . import Batch
         from . import workloads
         self._Batch, self._wl = Batch, workloads
         self.keep, self.precision = keep, precision
+        self.device_init = device_init  # initial state built on the GPU
         self._batch, self._members = None, ()
         self._next, self._next_members = None, ()
         self._fp = {}
@@ -241,6 +242,8 @@ class GpuEngine:
         return self.__dict__.setdefault(f"{name}_{threading.get_ident()}", {})
 
     def create(self, job):
+        if self.device_init:
+            return self._wl.build(job, self.precision, device_init=True)
         return self._wl.build(job, self.precision, host=self._buffers("init"))
 
     def _build(self, members):

@@ -110,13 +110,18 @@ def served_stream(count=160, rate=50.0, seed=5150, tol=MIXED_TOLERANCE):
     return jobs
 
 
-def build(job: Job, precision=None, host=None) -> Instance:
+def build(job: Job, precision=None, host=None, device_init=False) -> Instance:
     """Creates, initialises and prepares the instance of a job.  ``host``
     (a dict) keeps the host arrays of the initial state for reuse by later
-    jobs of the same grid shape."""
+    jobs of the same grid shape; ``device_init`` builds the initial state on
+    the device instead (no host arrays, no upload)."""
     prec = job.precision if precision is None else precision
     inst = Instance(job.n, *job.coords(), coord=COORD_CARTESIAN, bc=job.bc, precision=prec,
                     gamma=job.gamma)
+    if device_init:
+        inst.init_problem_device(job.kind, **job.over)
+        inst.prepare()
+        return inst
     out = None
     if host is not None:
         if inst.N not in host:

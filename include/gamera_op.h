@@ -211,6 +211,16 @@ void gop_problem_defaults(int kind, gop_problem *p);
  * (src/main.c:57-61). */
 int gop_problem_init(const gop_desc *desc, const gop_problem *p, double *gas, double *face_b);
 
+/* The same initial state built on the device, directly in h's current state
+ * (what gop_problem_init followed by gop_upload(h, gas, face_b, NULL, NULL,
+ * 0, 0) leaves, to the last bits of the device's sin/cos/exp/acos/atan2):
+ * cells, then for the potential problems AinitB's edge integrals
+ * (src/solver_func.c:15-95, in the instance's work arrays as scratch) and
+ * the face field.  gop_prepare follows as after gop_upload.  GOP_EINVAL if
+ * the problem does not fit the instance's geometry.  The reference builds
+ * its initial state on the host (problem_init). */
+int gop_problem_init_device(gop_instance *h, const gop_problem *p);
+
 /* ---- batched stepping of many independent instances ---------------- */
 typedef struct gop_batch gop_batch;
 

@@ -47,14 +47,14 @@ def test_served_results_equal_alone_and_within_tolerance_of_fp64(gop):
     pool = {}
     for o, j in zip(rep.outcomes, jobs):
         assert o.rid == j.rid and o.result["steps"] == j.steps
-        alone = workloads.build(j)
+        alone = workloads.build(j, device_init=True)  # as the engine builds it
         alone.step(j.steps)
         a = serve.download_result(alone, pool, copy=True)
         alone.close()
         assert np.array_equal(o.result["gas"], a["gas"]), j
         assert np.array_equal(o.result["face_b"], a["face_b"]), j
         assert o.result["time"] == a["time"]
-        ref = workloads.build(j, precision=gop.PREC_FP64)
+        ref = workloads.build(j, precision=gop.PREC_FP64, device_init=True)
         ref.step(j.steps)
         r = serve.download_result(ref, pool, copy=True)
         ref.close()
