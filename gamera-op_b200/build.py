@@ -18,6 +18,7 @@ SOURCES = [
     PKG / "csrc" / "gop_noalloc.cu",
     PKG / "csrc" / "gop_init.cu",
     PKG / "host" / "gop_problems.c",
+    PKG / "host" / "gop_background.c",
 ]
 HEADERS = [ROOT / "include" / "gamera_op.h", PKG / "csrc" / "gop_device.cuh",
            PKG / "csrc" / "gop_kernels.h", PKG / "csrc" / "gop_internal.h",

@@ -346,6 +346,7 @@ struct gop_instance {
   float* tabf = nullptr;     // FP32 copy of the tables (mixed path)
   double* scal = nullptr;
   double* staging = nullptr; // reference-layout scratch, 6 x NI*NJ*NK
+  double* bg = nullptr;      // background field block (BG_NF fields), if set
   double* hscal = nullptr;   // host copy of the scalars
   Work<double> wd;
   Work<float> wf;
@@ -551,7 +552,7 @@ int gop_destroy(gop_instance* h) {
   if (h->st) cudaStreamSynchronize(h->st);
   drop_step_graph(h);
   for (void* p : {(void*)h->state, h->work, (void*)h->tab, (void*)h->tabf, (void*)h->scal,
-                  (void*)h->staging})
+                  (void*)h->staging, (void*)h->bg})
     if (p) cudaFreeAsync(p, h->st);
   if (h->own) cudaStreamDestroy(h->own);  // released once the frees have run
   delete[] h->hscal;
@@ -595,6 +596,48 @@ int gop_upload(gop_instance* h, const double* gas, const double* face_b, const d
   CK(cudaMemcpyAsync(h->scal, s, NSCAL * sizeof(double), cudaMemcpyHostToDevice, h->st));
   CK(cudaStreamSynchronize(h->st));
   h->prepared = false;
+  return GOP_OK;
+}
+
+int gop_set_background(gop_instance* h, const double* b0, const double* lorentz,
+                       const double* b0_face, const double* b0_edge) {
+  if (!h) return fail(GOP_EINVAL, "instance is NULL");
+  const int given = (b0 != nullptr) + (lorentz != nullptr) + (b0_face != nullptr) + (b0_edge != nullptr);
+  if (given != 0 && given != 4) return fail(GOP_EINVAL, "the four background arrays go together");
+  Params& P = h->P;
+  drop_step_graph(h);  // the captured step has the other kernel set
+  h->prepared = false;
+  if (given == 0) {
+    if (h->bg) cudaFreeAsync(h->bg, h->st);
+    h->bg = nullptr;
+    P.bg = nullptr;
+    CK(cudaStreamSynchronize(h->st));
+    return GOP_OK;
+  }
+  if (!h->bg) {
+    cudaError_t e = cudaMallocAsync((void**)&h->bg, (size_t)P.fs * BG_NF * sizeof(double), h->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      h->bg = nullptr;
+      return fail(GOP_ENOMEM, "background allocation failed: %s", cudaGetErrorString(e));
+    }
+    h->bytes += (size_t)P.fs * BG_NF * sizeof(double);
+  }
+  CK(cudaMemsetAsync(h->bg, 0, (size_t)P.fs * BG_NF * sizeof(double), h->st));
+  const size_t ref = (size_t)P.N[0] * P.N[1] * P.N[2];
+  // through the staging buffer (6 fields) in groups of 3
+  const double* src[8] = {b0, lorentz, b0_face, b0_face + 3 * ref, b0_face + 6 * ref,
+                          b0_edge, b0_edge + 3 * ref, b0_edge + 6 * ref};
+  const int dst[8] = {BG_B0, BG_LOR, BG_FACE, BG_FACE + 3, BG_FACE + 6,
+                      BG_EDGE, BG_EDGE + 3, BG_EDGE + 6};
+  for (int g = 0; g < 8; g++) {
+    CK(cudaMemcpyAsync(h->staging, src[g], 3 * ref * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    launch_from_ref(P, 3, h->staging, h->bg + (size_t)dst[g] * P.fs, h->st);
+  }
+  CK(cudaStreamSynchronize(h->st));
+  CK(cudaGetLastError());
+  P.bg = h->bg;
   return GOP_OK;
 }
 

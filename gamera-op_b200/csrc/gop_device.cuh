@@ -84,7 +84,15 @@ struct Params {
   double* scal;           // device scalars
   double* Wbuf[2];        // two 6-field primitive buffers (current / next)
   double* Bbuf[2];        // two 3-field face-B buffers
+  const double* bg;       // background field block (BG_NF fields) or null
 };
+
+// Background field B0 (src/solver_func.c:1851-2077), BG_NF fields of the
+// state's layout: B0 at the cell centre (B0_b1..3), the Lorentz force of B0
+// (dmagsf_G), B0 averaged over the faces normal to axis d (B0Aface*_b1..3,
+// field BG_FACE + 3d + c) and along the edges of axis d (B0Aedge*_b1..3,
+// field BG_EDGE + 3d + c).
+enum BgField : int { BG_B0 = 0, BG_LOR = 3, BG_FACE = 6, BG_EDGE = 15, BG_NF = 24 };
 
 __device__ __forceinline__ int cur_buf(const Params& P) { return P.scal[S_PAR] != 0.0 ? 1 : 0; }
 

@@ -263,7 +263,7 @@ __device__ __forceinline__ void c2c_body(const Params& P, const Work<R>& wk, Pos
 
 // Second sweep, face-field reconstruction and the edge EMF
 // (src/solver_func.c:779-902) for edges along D: D active, p and q faces.
-template <typename R, int D>
+template <typename R, int D, bool BG>
 __device__ __forceinline__ void emf_body(const Params& P, const Work<R>& wk, Pos t) {
   constexpr int p = (D + 1) % 3, q = (D + 2) % 3;
   const int ijk[3] = {t.x, t.y, t.z};
@@ -308,7 +308,11 @@ __device__ __forceinline__ void emf_body(const Params& P, const Work<R>& wk, Pos
     for (int u = 0; u < 4; u++) lim[u] = B[q * fs + (u - 2) * sp];
     recon_lr<R>(v, lim, Wt, a1h, a2, bql, bqr);
   }
-  const R bp = R(0.5) * (bpl + bpr), bq = R(0.5) * (bql + bqr);
+  R bp = R(0.5) * (bpl + bpr), bq = R(0.5) * (bql + bqr);
+  if constexpr (BG) {  // + B0 averaged along the edge (B0Aedge*)
+    bp += (R)P.bg[(size_t)(BG_EDGE + 3 * D + p) * fs + x];
+    bq += (R)P.bg[(size_t)(BG_EDGE + 3 * D + q) * fs + x];
+  }
   const R vp = vav[0], vq = vav[1];
   R e = -(vp * bq - vq * bp);
   const R* rh = wk.Wh + x;  // density slot
@@ -328,11 +332,18 @@ __device__ __forceinline__ void emf_body(const Params& P, const Work<R>& wk, Pos
 // from the reconstructed states (src/solver_func.c:934-1529).  F[9] =
 // mass, 3 momenta, energy, entropy, 3 stress components.  Also writes the
 // first centre-to-edge sweep of edges along (D+2)%3 (see c2c_body).
-template <typename R, int D>
+template <typename R, int D, bool BG>
 __device__ __forceinline__ void flux_out(const Params& P, const Work<R>& wk, long long x,
                                          const R L[6], const R Rt[6], const R mL[3],
                                          const R mR[3]) {
   const size_t fs = P.fs;
+  // background field averaged over this face (B0Aface*_b1..3; the normal
+  // component is B0Aface*_bn)
+  R b0[3] = {R(0), R(0), R(0)};
+  if constexpr (BG) {
+#pragma unroll
+    for (int a = 0; a < 3; a++) b0[a] = (R)P.bg[(size_t)(BG_FACE + 3 * D + a) * fs + x];
+  }
   const R gm = (R)P.gamma, gm1 = (R)P.gm1, ca = (R)P.ca, ca2 = (R)P.ca2;
   const R rl = L[RHO], rr = Rt[RHO], pl = L[PR], pr = Rt[PR], sl = L[PS], sr = Rt[PS];
   const R irl = R(1) / rl, irr = R(1) / rr;
@@ -342,7 +353,16 @@ __device__ __forceinline__ void flux_out(const Params& P, const Work<R>& wk, lon
 
   const R btl = mL[0] * mL[0] + mL[1] * mL[1] + mL[2] * mL[2];
   const R btr = mR[0] * mR[0] + mR[1] * mR[1] + mR[2] * mR[2];
-  const R val = sqrt(btl * irl), var = sqrt(btr * irr);
+  // |B + B0|^2 of either state: the Alfven speed and the Boris term see the
+  // total field
+  R ttl = btl, ttr = btr;
+  if constexpr (BG) {
+    ttl = (mL[0] + b0[0]) * (mL[0] + b0[0]) + (mL[1] + b0[1]) * (mL[1] + b0[1]) +
+          (mL[2] + b0[2]) * (mL[2] + b0[2]);
+    ttr = (mR[0] + b0[0]) * (mR[0] + b0[0]) + (mR[1] + b0[1]) * (mR[1] + b0[1]) +
+          (mR[2] + b0[2]) * (mR[2] + b0[2]);
+  }
+  const R val = sqrt(ttl * irl), var = sqrt(ttr * irr);
   const R vel = val * ca * rsq(val * val + ca2);
   const R ver = var * ca * rsq(var * var + ca2);
   const R vnl = L[V1 + D], vnr = Rt[V1 + D];
@@ -386,23 +406,37 @@ __device__ __forceinline__ void flux_out(const Params& P, const Work<R>& wk, lon
   }
   o[5 * fs] = fS;
   const R bn = lim_b<R>(P, wk)[x + D * fs];
-  const R bq = (btl + btr) * (R)P.q_ca;
+  const R bq = (ttl + ttr) * (R)P.q_ca;
+  if constexpr (BG) {
+    // stress of B^2 + 2 B.B0 with the B0 cross terms
+    // (src/solver_func.c:1268-1333)
+    const R bsl = btl + R(2) * (mL[0] * b0[0] + mL[1] * b0[1] + mL[2] * b0[2]);
+    const R bsr = btr + R(2) * (mR[0] * b0[0] + mR[1] * b0[1] + mR[2] * b0[2]);
 #pragma unroll
-  for (int a = 0; a < 3; a++) {
-    R tl, tr;
-    if (a == D) {
-      tl = R(0.5) * (R(0.5) * btl - mL[a] * bn);
-      tr = R(0.5) * (R(0.5) * btr - mR[a] * bn);
-    } else {
-      tl = R(0.5) * (-mL[a] * bn);
-      tr = R(0.5) * (-mR[a] * bn);
+    for (int a = 0; a < 3; a++) {
+      const R pl = a == D ? R(0.5) * bsl : R(0), pr = a == D ? R(0.5) * bsr : R(0);
+      const R tl = R(0.5) * (pl - (mL[a] + b0[a]) * bn - mL[a] * b0[D]);
+      const R tr = R(0.5) * (pr - (mR[a] + b0[a]) * bn - mR[a] * b0[D]);
+      o[(6 + a) * fs] = (tl + tr) - bq * (Rt[V1 + a] - L[V1 + a]);
     }
-    o[(6 + a) * fs] = (tl + tr) - bq * (Rt[V1 + a] - L[V1 + a]);
+  } else {
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      R tl, tr;
+      if (a == D) {
+        tl = R(0.5) * (R(0.5) * btl - mL[a] * bn);
+        tr = R(0.5) * (R(0.5) * btr - mR[a] * bn);
+      } else {
+        tl = R(0.5) * (-mL[a] * bn);
+        tr = R(0.5) * (-mR[a] * bn);
+      }
+      o[(6 + a) * fs] = (tl + tr) - bq * (Rt[V1 + a] - L[V1 + a]);
+    }
   }
 }
 
 // PDM reconstruction of the 9 face states, then flux_out: one thread per face
-template <typename R, int D>
+template <typename R, int D, bool BG>
 __device__ __forceinline__ void flux_body(const Params& P, const Work<R>& wk, Pos t) {
   const int i = NGH + t.x, j = NGH + t.y, k = NGH + t.z;
   if (i >= NGH + P.n[0] + (D == 0) || j >= NGH + P.n[1] + (D == 1) ||
@@ -433,7 +467,7 @@ __device__ __forceinline__ void flux_body(const Params& P, const Work<R>& wk, Po
     for (int u = 0; u < 4; u++) lim[u] = ms[(u - 2) * s];
     recon_lr<R>(v, lim, Wt, a1h, a2, mL[a], mR[a]);
   }
-  flux_out<R, D>(P, wk, x, L, Rt, mL, mR);
+  flux_out<R, D, BG>(P, wk, x, L, Rt, mL, mR);
 }
 
 // --------------------------------------------------------------- update
@@ -464,7 +498,7 @@ __device__ __forceinline__ double ct_face(const Params& P, const double* __restr
 // conservative update and the pressure recovery are FP64; with R = float
 // the flux divergence, the Alfven/Boris correction and the CFL estimate are
 // FP32.  Returns the cell's CFL dt and |div B| of the new state.
-template <typename R>
+template <typename R, bool BG>
 __device__ __forceinline__ void update_cart(const Params& P, const Work<R>& wk, Pos t,
                                             double& dtc, double& dbmax) {
   const int i = NGH + t.x, j = NGH + t.y, k = NGH + t.z;
@@ -510,17 +544,31 @@ __device__ __forceinline__ void update_cart(const Params& P, const Work<R>& wk, 
   if (i == NGH + P.n[0] - 1) Bn[x + 1] = bu[0];
   if (j == NGH + P.n[1] - 1) Bn[x + sj + fs] = bu[1];
   if (k == NGH + P.n[2] - 1) Bn[x + sk + 2 * fs] = bu[2];
-  {
+  if constexpr (BG) {  // div of B + B0 (face-normal B0, src/solver_func.c:324-343)
+    const double* f0 = P.bg + (size_t)BG_FACE * fs + x;
+    const double* f1 = P.bg + (size_t)(BG_FACE + 4) * fs + x;
+    const double* f2 = P.bg + (size_t)(BG_FACE + 8) * fs + x;
+    const double dvb = ((bu[0] + f0[1]) * A[0] - (bl[0] + f0[0]) * A[0]) * ivol +
+                       ((bu[1] + f1[sj]) * A[1] - (bl[1] + f1[0]) * A[1]) * ivol +
+                       ((bu[2] + f2[sk]) * A[2] - (bl[2] + f2[0]) * A[2]) * ivol;
+    dbmax = fabs(dvb);
+  } else {
     const double dvb = (bu[0] * A[0] - bl[0] * A[0]) * ivol + (bu[1] * A[1] - bl[1] * A[1]) * ivol +
                        (bu[2] * A[2] - bl[2] * A[2]) * ivol;
     dbmax = fabs(dvb);
+  }
+  // cell-centred B0 (magtot = mags + B0)
+  double c0[3] = {0.0, 0.0, 0.0};
+  if constexpr (BG) {
+#pragma unroll
+    for (int a = 0; a < 3; a++) c0[a] = P.bg[(size_t)(BG_B0 + a) * fs + x];
   }
   double mn[3], mt[3];
   mn[0] = bl[0] * tb(P, 0, T_MA, i) + bu[0] * tb(P, 0, T_MB, i);
   mn[1] = bl[1] * tb(P, 1, T_MA, j) + bu[1] * tb(P, 1, T_MB, j);
   mn[2] = bl[2] * tb(P, 2, T_MA, k) + bu[2] * tb(P, 2, T_MB, k);
 #pragma unroll
-  for (int a = 0; a < 3; a++) mt[a] = 0.5 * (mn[a] + mo[a]);
+  for (int a = 0; a < 3; a++) mt[a] = BG ? 0.5 * (mn[a] + mo[a]) + c0[a] : 0.5 * (mn[a] + mo[a]);
 
   // flux divergence: 6 hydro and 3 stress components (R arithmetic when
   // R = float; the reference's F_u A - F_l A over the volume otherwise)
@@ -540,6 +588,10 @@ __device__ __forceinline__ void update_cart(const Params& P, const Work<R>& wk, 
       if (m < 6) du[m] = d == 0 ? v : du[m] + v;
       else dm[m - 6] = d == 0 ? v : dm[m - 6] + v;
     }
+  }
+  if constexpr (BG) {  // + the Lorentz force of B0 (src/solver_solve.c:312-324)
+#pragma unroll
+    for (int a = 0; a < 3; a++) dm[a] += (R)P.bg[(size_t)(BG_LOR + a) * fs + x];
   }
 
   // U^n from W^n, conservative update, cons->prim in FP64
@@ -600,7 +652,8 @@ __device__ __forceinline__ void update_cart(const Params& P, const Work<R>& wk, 
   // CFL dt of the new state with magtot = mags^{n+1} (src/solver_func.c:255-298)
   {
     const R r = (R)rho, u = (R)vv[0], v = (R)vv[1], w = (R)vv[2];
-    const R bsq = (R)(mn[0] * mn[0] + mn[1] * mn[1] + mn[2] * mn[2]);
+    const double t0 = mn[0] + c0[0], t1 = mn[1] + c0[1], t2 = mn[2] + c0[2];
+    const R bsq = BG ? (R)(t0 * t0 + t1 * t1 + t2 * t2) : (R)(mn[0] * mn[0] + mn[1] * mn[1] + mn[2] * mn[2]);
     const R va = sqrt(bsq / r);
     const R vae = va * (R)P.ca / sqrt(va * va + (R)P.ca2);
     const R vf = sqrt(u * u + v * v + w * w);
@@ -613,11 +666,11 @@ __device__ __forceinline__ void update_cart(const Params& P, const Work<R>& wk, 
 }
 
 // one active cell: returns its CFL dt and |div B| of the new state
-template <int COORD, typename R>
+template <int COORD, typename R, bool BG>
 __device__ __forceinline__ void update_body(const Params& P, const Work<R>& wk, Pos t,
                                             double& dtc, double& dbmax) {
   if constexpr (COORD == 0) {
-    update_cart<R>(P, wk, t, dtc, dbmax);
+    update_cart<R, BG>(P, wk, t, dtc, dbmax);
     return;
   }
   const int i = NGH + t.x, j = NGH + t.y, k = NGH + t.z;
@@ -653,6 +706,10 @@ __device__ __forceinline__ void update_body(const Params& P, const Work<R>& wk, 
       dm[a] = d == 0 ? v : dm[a] + v;
     }
   }
+  if constexpr (BG) {  // + the Lorentz force of B0 (src/solver_solve.c:312-324)
+#pragma unroll
+    for (int a = 0; a < 3; a++) dm[a] += P.bg[(size_t)(BG_LOR + a) * fs + x];
+  }
   // spherical geometric sources (src/spherical/spherical_general.c:605-681)
   double sh[3] = {0.0, 0.0, 0.0}, sb[3] = {0.0, 0.0, 0.0};
   if (COORD == 2) {
@@ -672,8 +729,15 @@ __device__ __forceinline__ void update_body(const Params& P, const Work<R>& wk, 
     sh[2] += -((double)Fj[3 * fs] * fj0 + (double)Fj[sjj + 3 * fs] * fj1) * sr;
     const R* Msh = wk.Msh + x;
     const double b1 = Msh[0], b2 = Msh[fs], b3 = Msh[2 * fs];
-    const double bsq = b1 * b1 + b2 * b2 + b3 * b3;
-    const double n22 = 0.5 * bsq - b2 * b2, n33 = 0.5 * bsq - b3 * b3;
+    double bsq = b1 * b1 + b2 * b2 + b3 * b3;
+    double n22 = 0.5 * bsq - b2 * b2, n33 = 0.5 * bsq - b3 * b3;
+    if constexpr (BG) {  // with the B0 cross terms (spherical_general.c:634-638)
+      const double* c0 = P.bg + (size_t)BG_B0 * fs + x;
+      const double g1 = c0[0], g2 = c0[fs], g3 = c0[2 * fs];
+      bsq = b1 * b1 + b2 * b2 + b3 * b3 + 2 * (b1 * g1 + b2 * g2 + b3 * g3);
+      n22 = 0.5 * bsq - (b2 + g2) * b2 - b2 * g2;
+      n33 = 0.5 * bsq - (b3 + g3) * b3 - b3 * g3;
+    }
     sb[0] = 0.5 * (n22 + n33) * (fi1 - fi0) * ivol;
     sb[1] = -((double)Fi[7 * fs] * fi0 + (double)Fi[si + 7 * fs] * fi1) * geo + (fj1 - fj0) * ivol * n33;
     sb[2] = -((double)Fi[8 * fs] * fi0 + (double)Fi[si + 8 * fs] * fi1) * geo;
@@ -730,6 +794,11 @@ __device__ __forceinline__ void update_body(const Params& P, const Work<R>& wk, 
     const int idx = a == 0 ? i : (a == 1 ? j : k);
     mn[a] = bl[a] * tb(P, a, T_MA, idx) + bu[a] * tb(P, a, T_MB, idx);
     mt[a] = 0.5 * (mn[a] + mags_at(P, B, a, i, j, k));
+    if constexpr (BG) {  // magtot = mags + B0
+      const double c0 = P.bg[(size_t)(BG_B0 + a) * fs + x];
+      mt[a] += c0;
+      mn[a] += c0;  // the next step's magtot, for its CFL dt
+    }
   }
   const double bsq = mt[0] * mt[0] + mt[1] * mt[1] + mt[2] * mt[2];
   const double alf = bsq / rho / P.ca2;
@@ -755,23 +824,38 @@ __device__ __forceinline__ void update_body(const Params& P, const Work<R>& wk, 
   Wn[x + 5 * fs] = pS;
   // CFL dt of the new state (magtot = mags^{n+1}) and max|div B^{n+1}|
   dtc = cfl_cell<COORD>(P, i, j, k, rho, vv[0], vv[1], vv[2], p, mn[0], mn[1], mn[2]);
-  const double dvb = (bu[0] * fu[0] - bl[0] * fl[0]) * ivol + (bu[1] * fu[1] - bl[1] * fl[1]) * ivol +
-                     (bu[2] * fu[2] - bl[2] * fl[2]) * ivol;
+  double b0l[3] = {0.0, 0.0, 0.0}, b0u[3] = {0.0, 0.0, 0.0};
+  if constexpr (BG) {  // div of B + B0 (face-normal B0, src/solver_func.c:324-343)
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const double* f = P.bg + (size_t)(BG_FACE + 4 * a) * fs + x;
+      b0l[a] = f[0];
+      b0u[a] = f[stride(P, a)];
+    }
+  }
+  const double dvb = ((bu[0] + b0u[0]) * fu[0] - (bl[0] + b0l[0]) * fl[0]) * ivol +
+                     ((bu[1] + b0u[1]) * fu[1] - (bl[1] + b0l[1]) * fl[1]) * ivol +
+                     ((bu[2] + b0u[2]) * fu[2] - (bl[2] + b0l[2]) * fl[2]) * ivol;
   dbmax = fabs(dvb);
   if (!(dtc > 0.0) || !isfinite(p) || !isfinite(rho) || !isfinite(vv[0] + vv[1] + vv[2]))
     P.scal[S_FLAGS] = 1.0;
 }
 
 // CFL dt and |div B| of one cell of the current state (prepare)
-template <int COORD>
+template <int COORD, bool BG>
 __device__ __forceinline__ void dt_body(const Params& P, Pos t, double& dtc, double& db) {
   const int i = NGH + t.x, j = NGH + t.y, k = NGH + t.z;
   if (i >= NGH + P.n[0] || j >= NGH + P.n[1] || k >= NGH + P.n[2]) return;
   const double* __restrict__ W = P.Wbuf[cur_buf(P)];
   const double* __restrict__ B = P.Bbuf[cur_buf(P)];
   const long long c = lin(P, i, j, k);
-  const double b1 = mags_at(P, B, 0, i, j, k), b2 = mags_at(P, B, 1, i, j, k),
-               b3 = mags_at(P, B, 2, i, j, k);
+  double b1 = mags_at(P, B, 0, i, j, k), b2 = mags_at(P, B, 1, i, j, k),
+         b3 = mags_at(P, B, 2, i, j, k);
+  if constexpr (BG) {  // magtot = mags + B0 (src/solver_func.c:345-353)
+    b1 += P.bg[(size_t)BG_B0 * P.fs + c];
+    b2 += P.bg[(size_t)(BG_B0 + 1) * P.fs + c];
+    b3 += P.bg[(size_t)(BG_B0 + 2) * P.fs + c];
+  }
   dtc = cfl_cell<COORD>(P, i, j, k, W[c], W[c + P.fs], W[c + 2 * P.fs], W[c + 3 * P.fs],
                         W[c + 4 * P.fs], b1, b2, b3);
   const double vol = Geo<COORD>::vol(P, i, j, k);
@@ -781,7 +865,13 @@ __device__ __forceinline__ void dt_body(const Params& P, Pos t, double& dtc, dou
     const double* f = B + (size_t)a * P.fs;
     const long long s = stride(P, a);
     const int i1 = i + (a == 0), j1 = j + (a == 1), k1 = k + (a == 2);
-    d += (f[c + s] * Geo<COORD>::face(P, a, i1, j1, k1) - f[c] * Geo<COORD>::face(P, a, i, j, k)) / vol;
+    double bu = f[c + s], bl = f[c];
+    if constexpr (BG) {
+      const double* g = P.bg + (size_t)(BG_FACE + 4 * a) * P.fs;
+      bu += g[c + s];
+      bl += g[c];
+    }
+    d += (bu * Geo<COORD>::face(P, a, i1, j1, k1) - bl * Geo<COORD>::face(P, a, i, j, k)) / vol;
   }
   db = fabs(d);
 }
@@ -912,10 +1002,10 @@ __global__ void k_begin(Params P) { begin_body(P); }
 __global__ void k_end(Params P) { end_body(P); }
 __global__ void k_arm(Params P, double tstop, double budget) { arm_body(P, tstop, budget); }
 
-template <int COORD>
+template <int COORD, bool BG>
 __global__ void k_dt(Params P) {
   double dtc = DBL_MAX, db = 0.0;
-  dt_body<COORD>(P, grid_pos(), dtc, db);
+  dt_body<COORD, BG>(P, grid_pos(), dtc, db);
   block_commit(dtc, db, P.scal + S_NEXT_DT, P.scal + S_DIVB);
 }
 
@@ -929,21 +1019,22 @@ __global__ void __launch_bounds__(256, GOP_MINB(C2C, R)) k_c2c(Params P, Work<R>
   if (stopped(P)) return;
   c2c_body<R, D>(P, w, grid_pos());
 }
-template <typename R, int D>
+// BG: with the background-field terms (Params::bg set)
+template <typename R, int D, bool BG>
 __global__ void __launch_bounds__(256, GOP_MINB(EMF, R)) k_emf(Params P, Work<R> w) {
   if (stopped(P)) return;
-  emf_body<R, D>(P, w, grid_pos());
+  emf_body<R, D, BG>(P, w, grid_pos());
 }
-template <typename R, int D>
+template <typename R, int D, bool BG>
 __global__ void __launch_bounds__(256, GOP_MINB(FLUX, R)) k_flux(Params P, Work<R> w) {
   if (stopped(P)) return;
-  flux_body<R, D>(P, w, grid_pos());
+  flux_body<R, D, BG>(P, w, grid_pos());
 }
-template <int COORD, typename R>
+template <int COORD, typename R, bool BG>
 __global__ void __launch_bounds__(256, GOP_UPD_MINB(COORD, R)) k_update(Params P, Work<R> w) {
   if (stopped(P)) return;
   double dtc = DBL_MAX, db = 0.0;
-  update_body<COORD, R>(P, w, grid_pos(), dtc, db);
+  update_body<COORD, R, BG>(P, w, grid_pos(), dtc, db);
   block_commit(dtc, db, P.scal + S_NEXT_DT, P.scal + S_DIVB);
 }
 __global__ void k_wrap(Params P, int axis, int which) {
@@ -1061,13 +1152,19 @@ void launch_arm(const Params& P, double tstop, double budget, cudaStream_t st) {
 void launch_dt(const Params& P, int coord, cudaStream_t st) {
   const dim3 blk(32, 4, 2);
   const dim3 g = grid3(P.n[0], P.n[1], P.n[2], blk);
-  if (coord == 0) LAUNCH(k_dt<0>, g, blk, st, P);
-  else LAUNCH(k_dt<2>, g, blk, st, P);
+  const bool bg = P.bg != nullptr;
+  if (coord == 0) {
+    if (bg) LAUNCH((k_dt<0, true>), g, blk, st, P);
+    else LAUNCH((k_dt<0, false>), g, blk, st, P);
+  } else {
+    if (bg) LAUNCH((k_dt<2, true>), g, blk, st, P);
+    else LAUNCH((k_dt<2, false>), g, blk, st, P);
+  }
 }
 
-template <typename R>
-void launch_slot(const Params& P, int coord, const Work<R>& w, int slot, dim3 blk,
-                 cudaStream_t st) {
+template <typename R, bool BG>
+static void launch_slot_bg(const Params& P, int coord, const Work<R>& w, int slot, dim3 blk,
+                           cudaStream_t st) {
   const dim3 sp = launch_space(P, slot);
   const dim3 g = grid3(sp.x, sp.y, sp.z, blk);
   switch (slot) {
@@ -1075,18 +1172,25 @@ void launch_slot(const Params& P, int coord, const Work<R>& w, int slot, dim3 bl
     case K_C2C0: LAUNCH((k_c2c<R, 0>), g, blk, st, P, w); break;
     case K_C2C1: LAUNCH((k_c2c<R, 1>), g, blk, st, P, w); break;
     case K_C2C2: LAUNCH((k_c2c<R, 2>), g, blk, st, P, w); break;
-    case K_EMF0: LAUNCH((k_emf<R, 0>), g, blk, st, P, w); break;
-    case K_EMF1: LAUNCH((k_emf<R, 1>), g, blk, st, P, w); break;
-    case K_EMF2: LAUNCH((k_emf<R, 2>), g, blk, st, P, w); break;
-    case K_FLUX0: LAUNCH((k_flux<R, 0>), g, blk, st, P, w); break;
-    case K_FLUX1: LAUNCH((k_flux<R, 1>), g, blk, st, P, w); break;
-    case K_FLUX2: LAUNCH((k_flux<R, 2>), g, blk, st, P, w); break;
+    case K_EMF0: LAUNCH((k_emf<R, 0, BG>), g, blk, st, P, w); break;
+    case K_EMF1: LAUNCH((k_emf<R, 1, BG>), g, blk, st, P, w); break;
+    case K_EMF2: LAUNCH((k_emf<R, 2, BG>), g, blk, st, P, w); break;
+    case K_FLUX0: LAUNCH((k_flux<R, 0, BG>), g, blk, st, P, w); break;
+    case K_FLUX1: LAUNCH((k_flux<R, 1, BG>), g, blk, st, P, w); break;
+    case K_FLUX2: LAUNCH((k_flux<R, 2, BG>), g, blk, st, P, w); break;
     case K_UPDATE:
-      if (coord == 0) LAUNCH((k_update<0, R>), g, blk, st, P, w);
-      else LAUNCH((k_update<2, R>), g, blk, st, P, w);
+      if (coord == 0) LAUNCH((k_update<0, R, BG>), g, blk, st, P, w);
+      else LAUNCH((k_update<2, R, BG>), g, blk, st, P, w);
       break;
     default: break;
   }
+}
+
+template <typename R>
+void launch_slot(const Params& P, int coord, const Work<R>& w, int slot, dim3 blk,
+                 cudaStream_t st) {
+  if (P.bg) launch_slot_bg<R, true>(P, coord, w, slot, blk, st);
+  else launch_slot_bg<R, false>(P, coord, w, slot, blk, st);
 }
 
 template void launch_slot<double>(const Params&, int, const Work<double>&, int, dim3, cudaStream_t);

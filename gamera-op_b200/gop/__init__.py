@@ -64,6 +64,12 @@ class Problem(C.Structure):
     ]
 
 
+class Background(C.Structure):
+    _fields_ = [("kind", C.c_int), ("b", C.c_double * 3), ("moment", C.c_double)]
+
+
+BG_UNIFORM, BG_DIPOLE = 1, 2
+
 _lib = None
 
 
@@ -91,6 +97,8 @@ def lib():
         L.gop_problem_defaults.argtypes = [C.c_int, C.POINTER(Problem)]
         L.gop_problem_init.argtypes = [C.POINTER(Desc), C.POINTER(Problem), _dp, _dp]
         L.gop_problem_init_device.argtypes = [vp, C.POINTER(Problem)]
+        L.gop_set_background.argtypes = [vp, _dp, _dp, _dp, _dp]
+        L.gop_background_init.argtypes = [C.POINTER(Desc), C.POINTER(Background), _dp, _dp, _dp, _dp]
         L.gop_autotune.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
         L.gop_set_profiling.argtypes = [vp, C.c_int]
         L.gop_get_profile.argtypes = [vp, _dp, C.POINTER(C.c_int64)]
@@ -215,6 +223,21 @@ class Instance:
         init_problem + upload (gop_problem_init_device); prepare follows."""
         p = problem(kind, **over)
         _check(lib().gop_problem_init_device(self._h, C.byref(p)))
+
+    def background_fields(self, kind: int, b=(0.0, 0.0, 0.0), moment=1.0) -> dict:
+        """A built-in background field on this instance's grid (see the
+        module function background_fields)."""
+        return _background(self.desc, self.N, kind, b, moment)
+
+    def set_background(self, fields):
+        """Installs a background field (the arrays of background_fields, or
+        None to remove it); prepare must follow."""
+        if fields is None:
+            _check(lib().gop_set_background(self._h, None, None, None, None))
+            return
+        arr = [_contig(fields[k], self.shape(nf)) for k, nf in
+               (("b0", 3), ("lorentz", 3), ("b0_face", 9), ("b0_edge", 9))]
+        _check(lib().gop_set_background(self._h, *[_ptr(a) for a in arr]))
 
     def upload(self, gas, face_b, gas_p=None, face_b_p=None, time=0.0, dt0=0.0):
         gas = _contig(gas, self.shape(6))
@@ -347,6 +370,29 @@ def problem_state(n, xs, kind, coord=COORD_CARTESIAN, **over):
     p = problem(kind, **over)
     _check(lib().gop_problem_init(C.byref(d), C.byref(p), _ptr(gas), _ptr(fb)))
     return gas, fb
+
+
+def _background(desc, N, kind, b, moment):
+    bg = Background(kind, (C.c_double * 3)(*b), moment)
+    out = {"b0": np.zeros((3,) + N), "lorentz": np.zeros((3,) + N),
+           "b0_face": np.zeros((9,) + N), "b0_edge": np.zeros((9,) + N)}
+    _check(lib().gop_background_init(C.byref(desc), C.byref(bg), _ptr(out["b0"]),
+                                     _ptr(out["lorentz"]), _ptr(out["b0_face"]),
+                                     _ptr(out["b0_edge"])))
+    return out
+
+
+def background_fields(n, xs, kind, coord=COORD_CARTESIAN, b=(0.0, 0.0, 0.0), moment=1.0):
+    """Host-only: a built-in background field B0 (BG_UNIFORM with field b,
+    or BG_DIPOLE scaled by moment) integrated over a grid
+    (gop_background_init): arrays b0 (3 fields), lorentz (3), b0_face (9),
+    b0_edge (9), as Instance.set_background takes them."""
+    n = tuple(int(v) for v in n)
+    N = tuple(v + 2 * NG + 1 for v in n)
+    xs = [np.ascontiguousarray(x, dtype=np.float64) for x in xs]
+    d = Desc(n[0], n[1], n[2], coord, _ptr(xs[0]), _ptr(xs[1]), _ptr(xs[2]), b"pppppp",
+             b"", 0, 0, 0, 0, 0, 0)
+    return _background(d, N, kind, b, moment)
 
 
 def make(kind, n, domain=None, coord=None, bc="pppppp", precision=PREC_FP64, **over):

@@ -12,7 +12,8 @@
  * so the per-step files keep their layout.
  *
  * Supported: one domain (proc_dims 1x1x1), COORD_TYPE 0 or 2, the BC library
- * of src/boundary_conditions.c, B0 = 0 and no gravity (the supplied problems).
+ * of src/boundary_conditions.c, a background field B0 (the arrays main's
+ * set_background_field leaves in gem go to the device), no gravity.
  * Not supported: the spherical pole ring average (doRingAverage = 1).
  * GOP_PRECISION=mixed in the environment selects the mixed-precision stages.
  */
@@ -22,6 +23,7 @@
 
 #include <mpi.h>
 
+#include "common.h"
 #include "config.h"
 #include "curvilinear.h"
 #include "log.h"
@@ -110,6 +112,20 @@ int solve(int nt) {
   rc = gop_upload(h, gs, gm, read_restart ? gs + (gas_rho_p - gas_rho) * n3 : NULL,
                   read_restart ? gm + (mag_bi_p - mag_bi) * n3 : NULL, time_sim, dt0);
   if (rc) return gop_fail(h, "gop_upload", rc);
+  if (B10 != Field_Default || B20 != Field_Default || B30 != Field_Default) {
+    /* the background field set_background_field integrated on the host
+     * (src/main.c:63): cell B0, its Lorentz force and the edge averages are
+     * consecutive slots; the face averages b1..b3 are gathered per axis */
+    double *face = (double *)malloc(9 * n3 * sizeof(double));
+    if (!face) return gop_fail(h, "background staging", GOP_ENOMEM);
+    const int fslot[3] = {B0AfaceI_b1, B0AfaceJ_b1, B0AfaceK_b1};
+    for (int a = 0; a < 3; a++)
+      memcpy(face + 3 * a * n3, gm + (fslot[a] - mag_bi) * n3, 3 * n3 * sizeof(double));
+    rc = gop_set_background(h, gm + (B0_b1 - mag_bi) * n3, gm + (dmagsf_G_x1dir - mag_bi) * n3,
+                            face, gm + (B0AedgeI_b1 - mag_bi) * n3);
+    free(face);
+    if (rc) return gop_fail(h, "gop_set_background", rc);
+  }
   /* halo, boundary fill, derived variables and (fresh start) the AB2
    * history and initial dt0 (src/solver_solve.c:25-99) */
   rc = gop_prepare(h, read_restart ? 1 : 0);

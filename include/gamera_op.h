@@ -221,6 +221,43 @@ int gop_problem_init(const gop_desc *desc, const gop_problem *p, double *gas, do
  * its initial state on the host (problem_init). */
 int gop_problem_init_device(gop_instance *h, const gop_problem *p);
 
+/* ---- background magnetic field B0 ------------------------------------ */
+/* The reference adds a time-independent background field B0 (the problem
+ * sets its B10/B20/B30 hooks; set_background_field, src/solver_func.c:
+ * 1851-2077, integrates it once) to the face fluxes, the magnetic stress,
+ * the edge EMFs, the Alfven correction and the CFL dt.  Four groups of
+ * arrays describe it, each field [i][j][k] like gop_upload's:
+ *   b0       3 fields: B0 at the cell centroid (B0_b1..3)
+ *   lorentz  3 fields: the Lorentz force of B0 (dmagsf_G_x1..3dir)
+ *   b0_face  9 fields: field 3d+c = component c averaged over the faces
+ *            normal to axis d (B0AfaceI/J/K_b1..3)
+ *   b0_edge  9 fields: field 3d+c = component c averaged along the edges of
+ *            axis d (B0AedgeI/J/K_b1..3; active range only)
+ * gop_set_background installs them (all four, or all NULL to remove the
+ * background); gop_prepare must follow, and a batch must be created after
+ * it.  The instance then holds 24 more fields of doubles on the device than
+ * gop_footprint counts. */
+int gop_set_background(gop_instance *h, const double *b0, const double *lorentz,
+                       const double *b0_face, const double *b0_edge);
+
+#define GOP_BG_UNIFORM 1  /* constant b (src/common.c B10_uniform with b = 1/sqrt2) */
+#define GOP_BG_DIPOLE 2   /* moment * (3xz, 3yz, 2z^2-x^2-y^2) / r^5 (src/common.c
+                             B10_dipole with moment 1), evaluated on the grid's own
+                             coordinates as the reference does */
+typedef struct {
+  int kind;          /* GOP_BG_* */
+  double b[3];       /* uniform: the field */
+  double moment;     /* dipole: scale of the reference's unit dipole */
+} gop_background;
+
+/* set_background_field on the host for one of the built-in backgrounds (no
+ * volume source, as in every reference problem): the 12x12 Gauss face
+ * averages with the metric scale factors, the 12-point edge averages and
+ * the Lorentz force from the face stresses; arrays as gop_set_background
+ * takes them. */
+int gop_background_init(const gop_desc *desc, const gop_background *bg, double *b0,
+                        double *lorentz, double *b0_face, double *b0_edge);
+
 /* ---- batched stepping of many independent instances ---------------- */
 typedef struct gop_batch gop_batch;
 

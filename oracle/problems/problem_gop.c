@@ -19,6 +19,10 @@
  *           GOP_B "b1,b2,b3" (uniform face field)
  *   loop_sph: GOP_V "vx,vy,vz" (Cartesian), GOP_RHO, GOP_P, GOP_LOOP
  *           "xc,yc,R,A0"
+ *   GOP_B0   uniform | dipole: the background field hooks B10/B20/B30 of
+ *            src/common.c (B10_uniform..., B10_dipole...), integrated by the
+ *            reference's set_background_field after problem_init (default:
+ *            none)
  *
  * The Orszag-Tang and Cartesian field-loop initial states follow the
  * reference problems (src/problem_test_OT_cartesion.c:50-130,
@@ -190,9 +194,30 @@ static double loops_a3(double x1, double x2, double x3) {
   return a[2];
 }
 
+/* the reference's dipole hooks (src/common.c:30-41; not declared in its
+ * headers) */
+double B10_dipole(double x, double y, double z);
+double B20_dipole(double x, double y, double z);
+double B30_dipole(double x, double y, double z);
+
+static void select_background(void) {
+  const char *s = getenv("GOP_B0");
+  if (!s) return;
+  if (strcmp(s, "uniform") == 0) {
+    B10 = B10_uniform;
+    B20 = B20_uniform;
+    B30 = B30_uniform;
+  } else if (strcmp(s, "dipole") == 0) {
+    B10 = B10_dipole;
+    B20 = B20_dipole;
+    B30 = B30_dipole;
+  }
+}
+
 void problem_init() {
   const char *kind = problem_kind();
   log_info("Initializing GOP problem %s", kind);
+  select_background();
   Field b_none = Field_Default;
   if (strcmp(kind, "ot") == 0) {
     A3 = ot_az;

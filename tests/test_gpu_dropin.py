@@ -42,7 +42,16 @@ def _compare_dumps(a, b, n, tol):
          env={"GOP_CENTER": "0.1,-0.05,0.0", "GOP_B": "0.3,0.5,0.2"}),
     dict(n=(20, 16, 12), steps=25, problem="loop_sph", coord="sph", bc="eeeeee",
          env={"GOP_LOOP": "1.5,0,0.3,1e-3"}),
-])
+    # background fields B0: the reference's uniform and dipole hooks
+    dict(n=(16, 16, 12), steps=20, problem="blast", coord="cart", bc="pppppp",
+         env={"GOP_B0": "uniform"}),
+    dict(n=(16, 16, 12), steps=20, problem="blast", coord="cart", bc="eeeeee",
+         env={"GOP_B0": "dipole", "GOP_DOMAIN": "1.0,2.0,-0.5,0.5,-0.5,0.5",
+              "GOP_CENTER": "1.5,0.0,0.0", "GOP_B": "0,0,0"}),
+    dict(n=(20, 16, 12), steps=20, problem="loop_sph", coord="sph", bc="eeeeee",
+         env={"GOP_B0": "dipole", "GOP_LOOP": "1.5,0,0.3,1e-3"}),
+], ids=["ot", "blast_mixed_bc", "loop_sph", "blast_b0_uniform", "blast_b0_dipole",
+        "loop_sph_b0_dipole"])
 def test_dropin_solve_matches_reference_program(case):
     c = case["coord"]
     _need(f"ref_{c}_strict", f"ref_{c}_gpu")
