@@ -17,6 +17,7 @@ SOURCES = [
     PKG / "csrc" / "gop_kernels.cu",
     PKG / "csrc" / "gop_noalloc.cu",
     PKG / "csrc" / "gop_init.cu",
+    PKG / "csrc" / "gop_ring.cu",
     PKG / "host" / "gop_problems.c",
     PKG / "host" / "gop_background.c",
 ]

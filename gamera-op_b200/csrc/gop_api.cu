@@ -298,20 +298,54 @@ int gop::check_desc(const gop_desc* d) {
   if (!d->x1 || !d->x2 || !d->x3) return fail(GOP_EINVAL, "coordinate arrays are NULL");
   for (int a = 0; a < 3; a++) {
     char lo = d->bc[2 * a], hi = d->bc[2 * a + 1];
-    if (!strchr("psrfen", lo) || !strchr("psrfen", hi) || lo == 0 || hi == 0)
+    // the pole fill only on the theta faces of a ring-averaged spherical grid
+    const char* kinds = (a == 1 && d->ring_average) ? "psrfeno" : "psrfen";
+    if (!strchr(kinds, lo) || !strchr(kinds, hi) || lo == 0 || hi == 0)
       return fail(GOP_EINVAL, "bad boundary kind on axis %d", a);
     if ((lo == 'p') != (hi == 'p'))
       return fail(GOP_EINVAL, "axis %d: periodic must be set on both faces", a);
     for (int s = 0; s < 2; s++) {
       char g = d->gem_bc[2 * a + s], b = d->bc[2 * a + s];
       if (g == 0) continue;
-      if (!strchr("psrfen", g)) return fail(GOP_EINVAL, "bad face-field boundary kind on axis %d", a);
+      if (!strchr(kinds, g)) return fail(GOP_EINVAL, "bad face-field boundary kind on axis %d", a);
       if ((g == 'p') != (b == 'p'))
         return fail(GOP_EINVAL, "axis %d: gas and face field disagree on periodicity", a);
     }
   }
   if (d->precision != GOP_PREC_FP64 && d->precision != GOP_PREC_MIXED)
     return fail(GOP_EINVAL, "precision must be GOP_PREC_FP64 or GOP_PREC_MIXED");
+  if (d->ring_average) {
+    RingSetup r;
+    if (ring_setup(d, r) != GOP_OK) return GOP_EINVAL;
+  }
+  return GOP_OK;
+}
+
+// set_RingAverage_config (src/spherical/spherical_RingAverage.c:54-150) for
+// one domain: the phi blocks of each ring row by nk, which poles the theta
+// range reaches, the ring rows per pole
+int gop::ring_setup(const gop_desc* d, RingSetup& r) {
+  r = RingSetup{};
+  if (d->coord != GOP_COORD_SPHERICAL) return fail(GOP_EINVAL, "the ring average needs a spherical grid");
+  static const int t256[16] = {8, 16, 32, 32, 64, 64, 64, 64, 128, 128, 128, 128, 128, 128, 128, 128};
+  int navr = 0;
+  switch (d->nk) {
+    case 256: navr = 16; break;
+    case 128: navr = 8; break;
+    case 64: navr = 4; break;
+    case 32: navr = 2; break;
+    default: return fail(GOP_EINVAL, "the ring average needs nk = 32, 64, 128 or 256");
+  }
+  for (int t = 0; t < navr; t++) r.nchunk[t] = t256[t];
+  if (d->bc[4] != 'p') return fail(GOP_EINVAL, "the ring average needs periodic k faces");
+  const double pi = 3.14159265358979323846;
+  if (fabs(d->x2[NGH]) < 1e-10) r.poles |= 1;
+  if (fabs(d->x2[NGH + d->nj] - pi) < 1e-10) r.poles |= 2;
+  r.jmax = d->nj - 1 < navr ? d->nj - 1 : navr - 1;
+  // the bands of the two poles (E rows jmax + 2 deep) must not meet
+  const int need = (r.poles == 3 ? 2 : 1) * (r.jmax + 2) + 1;
+  if (r.poles && d->nj < need)
+    return fail(GOP_EINVAL, "the ring average needs nj >= %d here", need);
   return GOP_OK;
 }
 
@@ -347,6 +381,7 @@ struct gop_instance {
   double* scal = nullptr;
   double* staging = nullptr; // reference-layout scratch, 6 x NI*NJ*NK
   double* bg = nullptr;      // background field block (BG_NF fields), if set
+  double* ringtab = nullptr; // pole ring average tables (Params::ringtab)
   double* hscal = nullptr;   // host copy of the scalars
   Work<double> wd;
   Work<float> wf;
@@ -537,7 +572,33 @@ int gop_create(const gop_desc* desc, gop_instance** out) {
                          w + 21 * L.fs, w + 24 * L.fs, nullptr, nullptr, h->tab,
                          h->tab + fw_offset(T.tmax)};
   }
-  cudaError_t le = cudaStreamSynchronize(h->st);
+  P.ring = 0;
+  if (d.ring_average) {
+    RingSetup r;
+    ring_setup(&d, r);  // validated by check_desc
+    const int nk = d.nk, n1 = L.N[1];
+    std::vector<double> rt(2 * nk + n1, 1.0);
+    const double pi = 3.14159265358979323846, dtheta = 2.0 * pi / nk;
+    for (int q = 0; q < nk; q++) {  // FilterBaseMode's phi angles
+      const double theta = dtheta * (q + 0.5);
+      rt[q] = std::cos(theta);
+      rt[nk + q] = std::sin(theta);
+    }
+    // dxk_ring = (nk / nchunk) dxk on the ring rows, negative pole last
+    for (int rr = 0; rr <= r.jmax; rr++) {
+      if (r.poles & 1) rt[2 * nk + NGH + rr] = (double)(nk / r.nchunk[rr]);
+      if (r.poles & 2) rt[2 * nk + NGH + d.nj - 1 - rr] = (double)(nk / r.nchunk[rr]);
+    }
+    alloc((void**)&h->ringtab, rt.size() * sizeof(double));
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(h->ringtab, rt.data(), rt.size() * sizeof(double), cudaMemcpyHostToDevice, h->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+    P.ring = r.poles;
+    P.ring_jmax = r.jmax;
+    for (int t = 0; t < 16; t++) P.nchunk[t] = r.nchunk[t];
+    P.ringtab = h->ringtab;
+  }
+  cudaError_t le = e != cudaSuccess ? e : cudaStreamSynchronize(h->st);
   if (le == cudaSuccess) le = cudaGetLastError();
   if (le != cudaSuccess) {
     gop_destroy(h);
@@ -552,7 +613,7 @@ int gop_destroy(gop_instance* h) {
   if (h->st) cudaStreamSynchronize(h->st);
   drop_step_graph(h);
   for (void* p : {(void*)h->state, h->work, (void*)h->tab, (void*)h->tabf, (void*)h->scal,
-                  (void*)h->staging, (void*)h->bg})
+                  (void*)h->staging, (void*)h->bg, (void*)h->ringtab})
     if (p) cudaFreeAsync(p, h->st);
   if (h->own) cudaStreamDestroy(h->own);  // released once the frees have run
   delete[] h->hscal;

@@ -85,6 +85,13 @@ struct Params {
   double* Wbuf[2];        // two 6-field primitive buffers (current / next)
   double* Bbuf[2];        // two 3-field face-B buffers
   const double* bg;       // background field block (BG_NF fields) or null
+  // pole ring average (spherical): bit 0 a pole at theta = 0 (j face NGH),
+  // bit 1 at theta = pi (j face NGH + nj); 0 off
+  int ring;
+  int ring_jmax;          // ring rows per pole - 1
+  int nchunk[16];         // phi blocks of ring row r
+  const double* ringtab;  // cos, sin of (k + 1/2) 2 pi / nk; then per j the
+                          // factor of the CFL length in phi (N[1] values)
 };
 
 // Background field B0 (src/solver_func.c:1851-2077), BG_NF fields of the

@@ -92,9 +92,20 @@ __device__ __forceinline__ double cfl_cell(const Params& P, int i, int j, int k,
   double vf = sqrt(u * u + v * v + w * w);
   double vs = sqrt(P.gamma * p / rho);
   double vc = vf + sqrt(vs * vs + vae * vae);
-  double t = vc / Geo<COORD>::dl(P, 0, i, j, k) + vc / Geo<COORD>::dl(P, 1, i, j, k) +
-             vc / Geo<COORD>::dl(P, 2, i, j, k);
+  double dk = Geo<COORD>::dl(P, 2, i, j, k);
+  // the phi length of the pole rings is nk / nchunk times longer (dxk_ring,
+  // spherical_RingAverage.c:110-138; get_dt_ring, spherical_general.c:700-743)
+  if (COORD == 2 && P.ring) dk = P.ringtab[2 * P.n[2] + j] * dk;
+  double t = vc / Geo<COORD>::dl(P, 0, i, j, k) + vc / Geo<COORD>::dl(P, 1, i, j, k) + vc / dk;
   return P.cfl / t;
+}
+
+// rows of cells whose state or face field the pole ring average changes
+// (the ring rows and the rows of the faces its EMF-like field touches)
+__device__ __forceinline__ bool ring_band_row(const Params& P, int j) {
+  const int jm = P.ring_jmax;
+  return ((P.ring & 1) && j >= NGH && j <= NGH + jm + 1) ||
+         ((P.ring & 2) && j >= NGH + P.n[1] - 2 - jm && j <= NGH + P.n[1] - 1);
 }
 
 // cell-centred B from the two faces along each axis (src/solver_func.c:311-322)
@@ -751,6 +762,16 @@ __device__ __forceinline__ void update_body(const Params& P, const Work<R>& wk, 
   bu[0] = ct_face<COORD, 0, R>(P, B, E, i + 1, j, k, dt);
   bu[1] = ct_face<COORD, 1, R>(P, B, E, i, j + 1, k, dt);
   bu[2] = ct_face<COORD, 2, R>(P, B, E, i, j, k + 1, dt);
+  if (COORD == 2 && P.ring) {
+    // B_j on a pole face (zero area) from the face next to it and the one
+    // half a turn away in phi (tackle_Magfield_pole,
+    // spherical_RingAverage.c:205-233)
+    const int ko = NGH + (k - NGH + P.n[2] / 2) % P.n[2];
+    if ((P.ring & 1) && j == NGH)
+      bl[1] = 0.5 * (bu[1] - ct_face<COORD, 1, R>(P, B, E, i, j + 1, ko, dt));
+    if ((P.ring & 2) && j == NGH + P.n[1] - 1)
+      bu[1] = 0.5 * (bl[1] - ct_face<COORD, 1, R>(P, B, E, i, j, ko, dt));
+  }
 #pragma unroll
   for (int a = 0; a < 3; a++) {
     Bn[x + a * fs] = bl[a];
@@ -839,6 +860,12 @@ __device__ __forceinline__ void update_body(const Params& P, const Work<R>& wk, 
   dbmax = fabs(dvb);
   if (!(dtc > 0.0) || !isfinite(p) || !isfinite(rho) || !isfinite(vv[0] + vv[1] + vv[2]))
     P.scal[S_FLAGS] = 1.0;
+  if (COORD == 2 && P.ring && ring_band_row(P, j)) {
+    // the ring average still changes this row: k_ring_dt takes its CFL dt
+    // and div B afterwards
+    dtc = DBL_MAX;
+    dbmax = 0.0;
+  }
 }
 
 // CFL dt and |div B| of one cell of the current state (prepare)
@@ -949,8 +976,15 @@ __device__ __forceinline__ void bcface_body(const Params& P, int axis, int side,
       if (kd == 'e') src = side == 0 ? NGH : N - 1 - NGH - 1 + onface;
       else src = side == 0 ? 2 * NGH - 1 - l + onface : N - 1 - NGH - 1 - l;
       ijk[axis] = src;
+      const int k0 = ijk[2];
+      // pole ('o', j faces): mirrored across the axis half a turn away in
+      // phi, the theta and phi components negated
+      // (src/spherical/spherical_boundary.c:23-138)
+      if (kd == 'o') ijk[2] = NGH + (k0 - NGH + P.n[2] / 2) % P.n[2];
       v = a[lin(P, ijk[0], ijk[1], ijk[2])];
+      ijk[2] = k0;
       if (kd == 'r' && gas && f == V1 + axis) v = -v;
+      if (kd == 'o' && (gas ? (f == V2 || f == V3) : f != 6)) v = -v;
     }
     ijk[axis] = dst;
     a[lin(P, ijk[0], ijk[1], ijk[2])] = v;
@@ -1006,6 +1040,51 @@ template <int COORD, bool BG>
 __global__ void k_dt(Params P) {
   double dtc = DBL_MAX, db = 0.0;
   dt_body<COORD, BG>(P, grid_pos(), dtc, db);
+  block_commit(dtc, db, P.scal + S_NEXT_DT, P.scal + S_DIVB);
+}
+
+// CFL dt and |div B| of the ring band rows of the new state, after the pole
+// ring average (get_derived_variables and get_dt_ring of the next step,
+// src/solver_func.c:308-343, src/spherical/spherical_general.c:700-743);
+// thread (i, band row, k)
+__global__ void k_ring_dt(Params P) {
+  double dtc = DBL_MAX, db = 0.0;
+  const int i = NGH + blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = NGH + blockIdx.z * blockDim.z + threadIdx.z;
+  const int slot = blockIdx.y * blockDim.y + threadIdx.y;
+  const int jm = P.ring_jmax, nrow = jm + 2, pole = slot / nrow, rr = slot % nrow;
+  const int j = pole == 0 ? NGH + rr : NGH + P.n[1] - 2 - jm + rr;
+  if (!stopped(P) && pole <= 1 && (P.ring & (1 << pole)) && i < NGH + P.n[0] &&
+      k < NGH + P.n[2]) {
+    const int nb = 1 - cur_buf(P);  // this step's result
+    const double* __restrict__ W = P.Wbuf[nb];
+    const double* __restrict__ B = P.Bbuf[nb];
+    const long long c = lin(P, i, j, k);
+    double b[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      b[a] = mags_at(P, B, a, i, j, k);
+      if (P.bg) b[a] += P.bg[(size_t)(BG_B0 + a) * P.fs + c];
+    }
+    dtc = cfl_cell<2>(P, i, j, k, W[c], W[c + P.fs], W[c + 2 * P.fs], W[c + 3 * P.fs],
+                      W[c + 4 * P.fs], b[0], b[1], b[2]);
+    const double vol = Geo<2>::vol(P, i, j, k);
+    double d = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const double* f = B + (size_t)a * P.fs;
+      const long long s = stride(P, a);
+      double bu = f[c + s], bl = f[c];
+      if (P.bg) {
+        const double* g = P.bg + (size_t)(BG_FACE + 4 * a) * P.fs;
+        bu += g[c + s];
+        bl += g[c];
+      }
+      const int i1 = i + (a == 0), j1 = j + (a == 1), k1 = k + (a == 2);
+      d += (bu * Geo<2>::face(P, a, i1, j1, k1) - bl * Geo<2>::face(P, a, i, j, k)) / vol;
+    }
+    db = fabs(d);
+  }
   block_commit(dtc, db, P.scal + S_NEXT_DT, P.scal + S_DIVB);
 }
 
@@ -1213,7 +1292,15 @@ void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t
     hook(g, 0);
   }
   hook(G_UPDATE, 1);
+  launch_pole_emf<R>(P, w, st);  // pole ring average only
   launch_slot<R>(P, coord, w, K_UPDATE, tune.blk[K_UPDATE], st);
+  // the work arrays are free after the update: 2 fields of doubles of scratch
+  if (P.ring) {
+    launch_ring_average(P, reinterpret_cast<double*>(w.Wh), st);
+    const int jm = P.ring_jmax;
+    const dim3 blk(32, 2, 4);
+    LAUNCH(k_ring_dt, grid3(P.n[0], 2 * (jm + 2), P.n[2], blk), blk, st, P);
+  }
   hook(G_UPDATE, 0);
 }
 

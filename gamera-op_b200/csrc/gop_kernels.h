@@ -80,6 +80,12 @@ void launch_to_ref(const Params& P, int nf, const double* src, double* dst, cuda
 template <typename R>
 void launch_widen(const Params& P, int nf, const R* src, double* dst, cudaStream_t st);
 void launch_mags(const Params& P, const double* B, double* out, cudaStream_t st);
+// pole ring average (spherical grids reaching a pole): the pole-edge EMFs
+// before the update; the ring averages of the new state after it (scratch:
+// 2 fields of doubles)
+template <typename R>
+void launch_pole_emf(const Params& P, const Work<R>& w, cudaStream_t st);
+void launch_ring_average(const Params& P, double* scratch, cudaStream_t st);
 // problem p's initial state in buffer 0 (cells, face field; ghosts left for
 // the ghost fill); scratch: 3 fields of doubles for the edge integrals
 void launch_problem_init(const Params& P, const gop_problem& p, int sph, double* scratch,

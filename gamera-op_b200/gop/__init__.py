@@ -45,6 +45,7 @@ class Desc(C.Structure):
         ("precision", C.c_int),
         ("gamma", C.c_double), ("cfl", C.c_double), ("ca", C.c_double),
         ("rho_floor", C.c_double), ("p_floor", C.c_double),
+        ("ring_average", C.c_int),
     ]
 
 
@@ -166,7 +167,7 @@ class Instance:
 
     def __init__(self, n, x1, x2, x3, coord=COORD_CARTESIAN, bc="pppppp",
                  precision=PREC_FP64, gamma=0.0, cfl=0.0, ca=0.0, rho_floor=0.0,
-                 p_floor=0.0, gem_bc=""):
+                 p_floor=0.0, gem_bc="", ring_average=False):
         self.n = tuple(int(v) for v in n)
         self.N = tuple(v + 2 * NG + 1 for v in self.n)
         self._x = [np.ascontiguousarray(x, dtype=np.float64) for x in (x1, x2, x3)]
@@ -174,7 +175,7 @@ class Instance:
         self.desc = Desc(self.n[0], self.n[1], self.n[2], coord,
                          _ptr(self._x[0]), _ptr(self._x[1]), _ptr(self._x[2]),
                          bc.encode(), gem_bc.encode(), precision, gamma, cfl, ca, rho_floor,
-                         p_floor)
+                         p_floor, int(bool(ring_average)))
         h = C.c_void_p()
         _check(lib().gop_create(C.byref(self.desc), C.byref(h)))
         self._h = h

@@ -52,3 +52,10 @@ GOP_BC_KIND(gem, gop_gem_bc, reflective, 'r')
 GOP_BC_KIND(gem, gop_gem_bc, fixed, 'f')
 GOP_BC_KIND(gem, gop_gem_bc, extrapolated, 'e')
 GOP_BC_KIND(gem, gop_gem_bc, none, 'n')
+
+/* the pole fills of spherical grids (src/spherical/spherical_boundary.c,
+ * theta faces only) */
+void gas_bc_pole_j_low(void) { gop_note(gop_gas_bc, 1, 0, 'o'); }
+void gas_bc_pole_j_high(void) { gop_note(gop_gas_bc, 1, 1, 'o'); }
+void gem_bc_pole_j_low(void) { gop_note(gop_gem_bc, 1, 0, 'o'); }
+void gem_bc_pole_j_high(void) { gop_note(gop_gem_bc, 1, 1, 'o'); }

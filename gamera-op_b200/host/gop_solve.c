@@ -13,8 +13,9 @@
  *
  * Supported: one domain (proc_dims 1x1x1), COORD_TYPE 0 or 2, the BC library
  * of src/boundary_conditions.c, a background field B0 (the arrays main's
- * set_background_field leaves in gem go to the device), no gravity.
- * Not supported: the spherical pole ring average (doRingAverage = 1).
+ * set_background_field leaves in gem go to the device), the spherical pole
+ * ring average (doRingAverage = 1, with the pole fills of
+ * spherical_boundary.c), no gravity.
  * GOP_PRECISION=mixed in the environment selects the mixed-precision stages.
  */
 #include <math.h>
@@ -59,10 +60,6 @@ static int gop_fail(gop_instance *h, const char *what, int rc) {
 }
 
 int solve(int nt) {
-  if (doRingAverage == 1) {
-    log_error("gop solve(): the spherical pole ring average is not supported");
-    return -1;
-  }
   if (config.proc_dims[0] * config.proc_dims[1] * config.proc_dims[2] != 1) {
     log_error("gop solve(): one domain per GPU instance (proc_dims 1 1 1)");
     return -1;
@@ -101,6 +98,7 @@ int solve(int nt) {
   d.ca = CA;
   d.rho_floor = rho_floor;
   d.p_floor = p_floor;
+  d.ring_average = doRingAverage == 1;
 
   gop_instance *h = NULL;
   int rc = gop_create(&d, &h);

@@ -49,6 +49,9 @@ extern "C" {
 #define GOP_BC_FIXED 'f'
 #define GOP_BC_EXTRAPOLATED 'e'
 #define GOP_BC_NONE 'n'
+#define GOP_BC_POLE 'o' /* spherical j faces on a pole (src/spherical/spherical_boundary.c):
+                           mirror across the axis with a half turn in phi; needs
+                           ring_average */
 
 /* arithmetic of the reconstruction / Riemann flux / edge-EMF stages */
 #define GOP_PREC_FP64 0  /* plain: everything in FP64 (reference parity) */
@@ -70,6 +73,15 @@ typedef struct {
   double ca;          /* Boris speed of light CA, 10 */
   double rho_floor;   /* 0.00316227 */
   double p_floor;     /* 0.000316227 */
+  /* doRingAverage (src/spherical/spherical_RingAverage.c): on a spherical grid
+   * whose theta range starts at 0 and/or ends at pi, the cells of the rings
+   * nearest each pole are averaged in phi after every update (block
+   * averages of nchunk(j) blocks with a parabolic profile), the face field
+   * by the equivalent flux correction, the E and B fields on the pole faces
+   * are fixed, and the CFL length in phi of those rings is scaled up.  nk
+   * must be 32, 64, 128 or 256 and cover the full phi circle with periodic k
+   * faces, and nj must leave room for both pole bands. */
+  int ring_average;
 } gop_desc;
 
 typedef struct {

@@ -13,7 +13,10 @@
  *   GOP_DOMAIN   "x1min,x1max,x2min,x2max,x3min,x3max"
  *   GOP_BC       6 letters for faces i-lo,i-hi,j-lo,j-hi,k-lo,k-hi:
  *                p periodic, s symmetric, r reflective, f fixed,
- *                e extrapolated, n none                 (default pppppp)
+ *                e extrapolated, n none, o pole (j faces of spherical
+ *                grids, src/spherical/spherical_boundary.c)
+ *                                                       (default pppppp)
+ *   GOP_RING     1: doRingAverage = 1 (the pole ring average)
  *   GOP_CA       Boris "speed of light" CA               (default 10)
  *   blast:  GOP_RHO, GOP_P_IN, GOP_P_OUT, GOP_RADIUS, GOP_CENTER "x,y,z",
  *           GOP_B "b1,b2,b3" (uniform face field)
@@ -91,7 +94,7 @@ void set_problem_config() {
   x3min_global = dom[4];
   x3max_global = dom[5];
   CA = env_d("GOP_CA", 10.0);
-  doRingAverage = 0;
+  doRingAverage = env_d("GOP_RING", 0.0) != 0.0 ? 1 : 0;
   problem_config.Boundary_i =
       (bc_letter(0) == 'p' && bc_letter(1) == 'p') ? BC_PERIODIC
                                                    : BC_NON_PERIODIC;
@@ -133,6 +136,18 @@ static void apply_face_bc(int face) {
        gem_bc_extrapolated_k_low, gem_bc_none_k_low},
       {gem_bc_symmetric_k_high, gem_bc_reflective_k_high, gem_bc_fixed_k_high,
        gem_bc_extrapolated_k_high, gem_bc_none_k_high}};
+#ifdef GOP_HAVE_POLE_BC
+  if (bc_letter(face) == 'o' && (face == 2 || face == 3)) {
+    if (face == 2) {
+      gas_bc_pole_j_low();
+      gem_bc_pole_j_low();
+    } else {
+      gas_bc_pole_j_high();
+      gem_bc_pole_j_high();
+    }
+    return;
+  }
+#endif
   int kind;
   switch (bc_letter(face)) {
     case 's': kind = 0; break;
