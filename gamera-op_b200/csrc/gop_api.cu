@@ -387,6 +387,7 @@ struct gop_instance {
   Work<float> wf;
   Tune tune;
   cudaGraphExec_t step_graph = nullptr;  // one captured step (replayed by gop_step)
+  uint64_t gen = 0;                      // bumped whenever a step's launches change
   int64_t step_nodes = 0;
   size_t bytes = 0;
   bool prepared = false;
@@ -440,9 +441,12 @@ static void prof_collect(gop_instance* h) {
   h->recs.clear();
 }
 
+// the launches of one step changed (kernel set, block shapes): the captured
+// step goes, and batches holding this instance capture theirs again
 static void drop_step_graph(gop_instance* h) {
   if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
   h->step_graph = nullptr;
+  h->gen++;
 }
 
 extern "C" {
@@ -573,6 +577,7 @@ int gop_create(const gop_desc* desc, gop_instance** out) {
                          h->tab + fw_offset(T.tmax)};
   }
   P.ring = 0;
+  P.ps_live = 1;  // until gop_prepare has looked
   if (d.ring_average) {
     RingSetup r;
     ring_setup(&d, r);  // validated by check_desc
@@ -755,11 +760,20 @@ int gop_prepare(gop_instance* h, int restart) {
   s[S_STEPS] = 0.0;
   s[S_FLAGS] = 0.0;
   s[S_PAR] = 0.0;
+  s[S_PSNZ] = 0.0;
   CK(cudaMemcpyAsync(h->scal, s, NSCAL * sizeof(double), cudaMemcpyHostToDevice, h->st));
   // CFL dt and div B of the initial state (src/solver_solve.c:94-98)
   launch_dt(P, h->d.coord, h->st);
+  // is the entropy channel live?  A p_S that is zero in the state and its
+  // history stays zero in every later step, and the flux kernels skip it
+  launch_ps_check(P, h->st);
   CK(cudaMemcpyAsync(s, h->scal, NSCAL * sizeof(double), cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
+  const int live = s[S_PSNZ] != 0.0 ? 1 : 0;
+  if (live != h->P.ps_live) {
+    drop_step_graph(h);
+    h->P.ps_live = live;
+  }
   if (!restart) s[S_DT0] = s[S_NEXT_DT];
   CK(cudaMemcpyAsync(h->scal, s, NSCAL * sizeof(double), cudaMemcpyHostToDevice, h->st));
   CK(cudaStreamSynchronize(h->st));
@@ -1062,6 +1076,7 @@ struct gop_batch {
   std::vector<cudaStream_t> br;  // branch streams (used while capturing)
   std::vector<cudaEvent_t> ev;   // fork and join events of the capture
   cudaGraphExec_t graph = nullptr;
+  std::vector<uint64_t> gen;     // the members' generations the graph holds
 };
 
 static void batch_release(gop_batch* b) {
@@ -1104,6 +1119,8 @@ static int batch_build(gop_batch* b) {
   // captured launches run at each replay, not now
   b->nodes = launches() - before;
   count_launches(-b->nodes);
+  b->gen.resize(b->m.size());
+  for (size_t i = 0; i < b->m.size(); i++) b->gen[i] = b->m[i]->gen;
   if (e == cudaSuccess) e = cudaGraphInstantiate(&b->graph, g, 0);
   if (g) cudaGraphDestroy(g);
   if (e != cudaSuccess) {
@@ -1220,6 +1237,16 @@ int gop_batch_launch(gop_batch* b, const int* steps) {
   // members' own streams may still hold work on their state
   for (gop_instance* h : b->m) CK(cudaStreamSynchronize(h->st));
   CK(cudaStreamSynchronize(b->st));  // the previous launch of this batch is done
+  // a member prepared again with another kernel set, background or block
+  // shapes: capture the step of all members again
+  for (size_t i = 0; i < b->m.size(); i++) {
+    if (!b->m[i]->prepared) return fail(GOP_ESTATE, "member %d is not prepared", (int)i);
+    if (b->m[i]->gen != b->gen[i]) {
+      const int rc = batch_build(b);
+      if (rc) return rc;
+      break;
+    }
+  }
   for (size_t i = 0; i < b->m.size(); i++) launch_arm(b->m[i]->P, 1e300, (double)steps[i], b->st);
   for (int n = 0; n < most; n++) CK(cudaGraphLaunch(b->graph, b->st));
   count_launches((int64_t)most * b->nodes);

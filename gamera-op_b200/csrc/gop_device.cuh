@@ -65,6 +65,8 @@ enum Scal : int {
   S_FLAGS,       // bit 0: non-finite / non-positive state seen
   S_PAR,         // which of the two state buffers holds the current state
   S_BUDGET,      // steps left in the current gop_step call
+  S_PSNZ,        // gop_prepare's check: nonzero if some p_S of the state or
+                 // of its AB2 history is nonzero
   NSCAL
 };
 
@@ -85,6 +87,10 @@ struct Params {
   double* Wbuf[2];        // two 6-field primitive buffers (current / next)
   double* Bbuf[2];        // two 3-field face-B buffers
   const double* bg;       // background field block (BG_NF fields) or null
+  // 1 if p_S (the entropy channel) is nonzero somewhere in the state or its
+  // AB2 history; 0 keeps it zero for good (zero states give a zero entropy
+  // flux and every fill copies), and the flux kernels skip it
+  int ps_live;
   // pole ring average (spherical): bit 0 a pole at theta = 0 (j face NGH),
   // bit 1 at theta = pi (j face NGH + nj); 0 off
   int ring;

@@ -26,6 +26,7 @@
 #include "gop_device.cuh"
 #include "gop_kernels.h"
 
+#include <algorithm>
 #include <atomic>
 #include <cfloat>
 
@@ -447,7 +448,8 @@ __device__ __forceinline__ void flux_out(const Params& P, const Work<R>& wk, lon
 }
 
 // PDM reconstruction of the 9 face states, then flux_out: one thread per face
-template <typename R, int D, bool BG>
+// (PSL: the entropy channel p_S is live, Params::ps_live)
+template <typename R, int D, bool BG, bool PSL>
 __device__ __forceinline__ void flux_body(const Params& P, const Work<R>& wk, Pos t) {
   const int i = NGH + t.x, j = NGH + t.y, k = NGH + t.z;
   if (i >= NGH + P.n[0] + (D == 0) || j >= NGH + P.n[1] + (D == 1) ||
@@ -461,8 +463,13 @@ __device__ __forceinline__ void flux_body(const Params& P, const Work<R>& wk, Po
   load_face_weights<D, R>(wk.tab, wk.fw, P.tmax, f, Wt);
   const R a1h = (R)(0.5 * P.pdm_a1), a2 = (R)P.pdm_a2;
   R L[6], Rt[6], mL[3], mR[3];
+  // PSL false: p_S is identically zero (Params::ps_live), its face states
+  // are zero and flux_out's zero path gives the zero entropy flux that
+  // reconstructing the zero line would give
+  L[PS] = Rt[PS] = R(0);
 #pragma unroll
   for (int m = 0; m < 6; m++) {
+    if (m == PS && !PSL) continue;
     R v[8], lim[4];
     line8<R, R>(wk.Wh + (size_t)m * fs + x, s, v);
 #pragma unroll
@@ -1036,6 +1043,18 @@ __global__ void k_begin(Params P) { begin_body(P); }
 __global__ void k_end(Params P) { end_body(P); }
 __global__ void k_arm(Params P, double tstop, double budget) { arm_body(P, tstop, budget); }
 
+// S_PSNZ <- 1 if p_S of either state buffer is nonzero at a point the AB2
+// stage reads (every point but the last plane of each axis)
+__global__ void k_ps_check(Params P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  bool nz = false;
+  if (i < P.N[0] - 1 && j < P.N[1] - 1 && k < P.N[2] - 1) {
+    const long long x = lin(P, i, j, k) + (long long)PS * P.fs;
+    nz = P.Wbuf[0][x] != 0.0 || P.Wbuf[1][x] != 0.0;
+  }
+  if (__any_sync(0xffffffffu, nz) && (threadIdx.x & 31) == 0) P.scal[S_PSNZ] = 1.0;
+}
+
 template <int COORD, bool BG>
 __global__ void k_dt(Params P) {
   double dtc = DBL_MAX, db = 0.0;
@@ -1104,10 +1123,10 @@ __global__ void __launch_bounds__(256, GOP_MINB(EMF, R)) k_emf(Params P, Work<R>
   if (stopped(P)) return;
   emf_body<R, D, BG>(P, w, grid_pos());
 }
-template <typename R, int D, bool BG>
+template <typename R, int D, bool BG, bool PSL>
 __global__ void __launch_bounds__(256, GOP_MINB(FLUX, R)) k_flux(Params P, Work<R> w) {
   if (stopped(P)) return;
-  flux_body<R, D, BG>(P, w, grid_pos());
+  flux_body<R, D, BG, PSL>(P, w, grid_pos());
 }
 template <int COORD, typename R, bool BG>
 __global__ void __launch_bounds__(256, GOP_UPD_MINB(COORD, R)) k_update(Params P, Work<R> w) {
@@ -1228,6 +1247,12 @@ void launch_arm(const Params& P, double tstop, double budget, cudaStream_t st) {
   LAUNCH(k_arm, 1, 1, st, P, tstop, budget);
 }
 
+void launch_ps_check(const Params& P, cudaStream_t st) {
+  const int nx = (P.N[0] - 1 + 31) / 32 * 32;
+  const dim3 blk(std::min(nx, 256), 1, 1);
+  LAUNCH(k_ps_check, dim3((nx + blk.x - 1) / blk.x, P.N[1] - 1, P.N[2] - 1), blk, st, P);
+}
+
 void launch_dt(const Params& P, int coord, cudaStream_t st) {
   const dim3 blk(32, 4, 2);
   const dim3 g = grid3(P.n[0], P.n[1], P.n[2], blk);
@@ -1254,9 +1279,18 @@ static void launch_slot_bg(const Params& P, int coord, const Work<R>& w, int slo
     case K_EMF0: LAUNCH((k_emf<R, 0, BG>), g, blk, st, P, w); break;
     case K_EMF1: LAUNCH((k_emf<R, 1, BG>), g, blk, st, P, w); break;
     case K_EMF2: LAUNCH((k_emf<R, 2, BG>), g, blk, st, P, w); break;
-    case K_FLUX0: LAUNCH((k_flux<R, 0, BG>), g, blk, st, P, w); break;
-    case K_FLUX1: LAUNCH((k_flux<R, 1, BG>), g, blk, st, P, w); break;
-    case K_FLUX2: LAUNCH((k_flux<R, 2, BG>), g, blk, st, P, w); break;
+    case K_FLUX0:
+      if (P.ps_live) LAUNCH((k_flux<R, 0, BG, true>), g, blk, st, P, w);
+      else LAUNCH((k_flux<R, 0, BG, false>), g, blk, st, P, w);
+      break;
+    case K_FLUX1:
+      if (P.ps_live) LAUNCH((k_flux<R, 1, BG, true>), g, blk, st, P, w);
+      else LAUNCH((k_flux<R, 1, BG, false>), g, blk, st, P, w);
+      break;
+    case K_FLUX2:
+      if (P.ps_live) LAUNCH((k_flux<R, 2, BG, true>), g, blk, st, P, w);
+      else LAUNCH((k_flux<R, 2, BG, false>), g, blk, st, P, w);
+      break;
     case K_UPDATE:
       if (coord == 0) LAUNCH((k_update<0, R, BG>), g, blk, st, P, w);
       else LAUNCH((k_update<2, R, BG>), g, blk, st, P, w);

@@ -69,6 +69,8 @@ void launch_end(const Params& P, cudaStream_t st);
 // arm a gop_step call: stop after time tstop or after `budget` steps
 void launch_arm(const Params& P, double tstop, double budget, cudaStream_t st);
 void launch_dt(const Params& P, int coord, cudaStream_t st);
+// P.scal[S_PSNZ] <- 1 if p_S is nonzero in either state buffer (it must be 0 before)
+void launch_ps_check(const Params& P, cudaStream_t st);
 template <typename R>
 void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t st,
                       const Tune& tune, const Hook& hook = Hook());

@@ -308,9 +308,12 @@ class Instance:
 
 class Batch:
     """Several prepared instances (any sizes, geometries, boundary kinds and
-    precisions) advanced together: every stage of a step is one launch over
-    the blocks of all members, and one captured batched step is replayed
-    max(steps) times; each member stops after its own step count."""
+    precisions) advanced together: one step of every member (its own launch
+    sequence) is captured in one CUDA graph on up to 16 parallel branches and
+    replayed max(steps) times; each member stops after its own step count.
+    A member prepared again with other kernels (a live entropy channel, a
+    background field, new block shapes) makes the next launch capture the
+    graph again."""
 
     def __init__(self, members):
         self.members = list(members)

@@ -22,6 +22,8 @@
  *           GOP_B "b1,b2,b3" (uniform face field)
  *   loop_sph: GOP_V "vx,vy,vz" (Cartesian), GOP_RHO, GOP_P, GOP_LOOP
  *           "xc,yc,R,A0"
+ *   GOP_PS   f: the entropy channel p_S = f * p in every initialised cell
+ *            (default 0: p_S stays 0, as in the reference's own problems)
  *   GOP_B0   uniform | dipole: the background field hooks B10/B20/B30 of
  *            src/common.c (B10_uniform..., B10_dipole...), integrated by the
  *            reference's set_background_field after problem_init (default:
@@ -316,5 +318,12 @@ void problem_init() {
       for (int j = js; j <= je; j++)
         for (int k = ks; k <= ke + 1; k++) gem[mag_bk][i][j][k] = b[2];
   }
+  double fps = env_d("GOP_PS", 0.0);
+  if (fps != 0.0)
+    for (int s = 0; s < NS1; s++)
+      for (int i = isg; i <= ieg; i++)
+        for (int j = jsg; j <= jeg; j++)
+          for (int k = ksg; k <= keg; k++)
+            gas[s][gas_p_S][i][j][k] = fps * gas[s][gas_p][i][j][k];
 }
 #endif
