@@ -742,8 +742,11 @@ int gop_problem_init_device(gop_instance* h, const gop_problem* p) {
 int gop_prepare(gop_instance* h, int restart) {
   if (!h) return fail(GOP_EINVAL, "instance is NULL");
   const Params& P = h->P;
-  // halo + boundary fill of the current state (src/solver_solve.c:25-40)
-  launch_ghosts(P, h->d.bc, h->d.gem_bc, 1, h->st);
+  // halo + boundary fill of the current state (src/solver_solve.c:25-40),
+  // every field: the state may be new
+  Params Pall = P;
+  Pall.ps_live = 1;
+  launch_ghosts(Pall, h->d.bc, h->d.gem_bc, 1, h->st);
   if (!restart) {
     // AB2 history <- current state (src/solver_solve.c:55-92)
     CK(cudaMemcpyAsync(P.Wbuf[1], P.Wbuf[0], (size_t)P.fs * 6 * sizeof(double),

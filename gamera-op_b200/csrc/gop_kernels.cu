@@ -194,8 +194,9 @@ __device__ __forceinline__ void arm_body(const Params& P, double tstop, double b
 // ------------------------------------------------------------------- AB2
 
 // W_h = W + c (W - W_old), mags and mags_h from the faces, B_h on faces
-// (src/solver_func.c:385-449) over the whole ghost-extended grid
-template <typename R>
+// (src/solver_func.c:385-449) over the whole ghost-extended grid; PSL false:
+// p_S and its extrapolation stay zero (Params::ps_live) and are not touched
+template <typename R, bool PSL>
 __device__ __forceinline__ void ab2_body(const Params& P, const Work<R>& w, Pos t) {
   const int i = t.x, j = t.y, k = t.z;
   if (i >= P.N[0] || j >= P.N[1] || k >= P.N[2]) return;
@@ -210,7 +211,7 @@ __device__ __forceinline__ void ab2_body(const Params& P, const Work<R>& w, Pos 
   const bool ci = i < P.N[0] - 1, cj = j < P.N[1] - 1, ck = k < P.N[2] - 1;
   if (ci && cj && ck) {
 #pragma unroll
-    for (int m = 0; m < 6; m++) {
+    for (int m = 0; m < (PSL ? 6 : 5); m++) {
       const double v = W[x + m * fs], vo = Wo[x + m * fs];
       w.Wh[x + m * fs] = (R)(v + c * (v - vo));
       if constexpr (sizeof(R) == 4) w.Wl[x + m * fs] = (R)v;
@@ -344,7 +345,7 @@ __device__ __forceinline__ void emf_body(const Params& P, const Work<R>& wk, Pos
 // from the reconstructed states (src/solver_func.c:934-1529).  F[9] =
 // mass, 3 momenta, energy, entropy, 3 stress components.  Also writes the
 // first centre-to-edge sweep of edges along (D+2)%3 (see c2c_body).
-template <typename R, int D, bool BG>
+template <typename R, int D, bool BG, bool PSL>
 __device__ __forceinline__ void flux_out(const Params& P, const Work<R>& wk, long long x,
                                          const R L[6], const R Rt[6], const R mL[3],
                                          const R mR[3]) {
@@ -416,7 +417,7 @@ __device__ __forceinline__ void flux_out(const Params& P, const Work<R>& wk, lon
     const R Sr = (sr == R(0) && rr > R(0)) ? sr : sr / pow(rr, gm1);
     fS = R(0.5) * (Sl * vnl + Sr * vnr - vfe * (Sr - Sl));
   }
-  o[5 * fs] = fS;
+  if constexpr (PSL) o[5 * fs] = fS;  // else the update takes a zero divergence
   const R bn = lim_b<R>(P, wk)[x + D * fs];
   const R bq = (ttl + ttr) * (R)P.q_ca;
   if constexpr (BG) {
@@ -485,7 +486,7 @@ __device__ __forceinline__ void flux_body(const Params& P, const Work<R>& wk, Po
     for (int u = 0; u < 4; u++) lim[u] = ms[(u - 2) * s];
     recon_lr<R>(v, lim, Wt, a1h, a2, mL[a], mR[a]);
   }
-  flux_out<R, D, BG>(P, wk, x, L, Rt, mL, mR);
+  flux_out<R, D, BG, PSL>(P, wk, x, L, Rt, mL, mR);
 }
 
 // --------------------------------------------------------------- update
@@ -516,7 +517,7 @@ __device__ __forceinline__ double ct_face(const Params& P, const double* __restr
 // conservative update and the pressure recovery are FP64; with R = float
 // the flux divergence, the Alfven/Boris correction and the CFL estimate are
 // FP32.  Returns the cell's CFL dt and |div B| of the new state.
-template <typename R, bool BG>
+template <typename R, bool BG, bool PSL>
 __device__ __forceinline__ void update_cart(const Params& P, const Work<R>& wk, Pos t,
                                             double& dtc, double& dbmax) {
   const int i = NGH + t.x, j = NGH + t.y, k = NGH + t.z;
@@ -597,6 +598,7 @@ __device__ __forceinline__ void update_cart(const Params& P, const Work<R>& wk, 
     const R* __restrict__ Fd = wk.F + (size_t)(9 * d) * fs + x;
 #pragma unroll
     for (int m = 0; m < 9; m++) {
+      if (m == PS && !PSL) continue;
       R v;
       if constexpr (sizeof(R) == 4) {
         v = (Fd[s + m * fs] - Fd[m * fs]) * (R)il[d];
@@ -616,21 +618,25 @@ __device__ __forceinline__ void update_cart(const Params& P, const Work<R>& wk, 
   // (src/solver_func.c:356-382, src/solver_solve.c:326-377)
   const double gm1 = P.gm1;
   const double r0 = W[x], u0 = W[x + fs], v0 = W[x + 2 * fs], w0 = W[x + 3 * fs],
-               p0 = W[x + 4 * fs], ps0 = W[x + 5 * fs];
+               p0 = W[x + 4 * fs];
   const double U0[3] = {r0 * u0, r0 * v0, r0 * w0};
   const double E0 = 0.5 * r0 * (u0 * u0 + v0 * v0 + w0 * w0) + p0 * P.inv_gm1;
-  const double S0 = (ps0 == 0.0 && r0 > 0.0) ? ps0 : ps0 / pow(r0, gm1);
   const double Ur = r0 - dt * (double)du[0];
   double Um[3];
 #pragma unroll
   for (int a = 0; a < 3; a++) Um[a] = U0[a] - dt * (double)du[1 + a];
   const double Ue = E0 - dt * (double)du[4];
-  const double Us = S0 - dt * (double)du[5];
   double rho = Ur;
   const double irho = 1.0 / Ur;
   double vv[3] = {Um[0] * irho, Um[1] * irho, Um[2] * irho};
   double p = (Ue - 0.5 * (vv[0] * vv[0] + vv[1] * vv[1] + vv[2] * vv[2]) * rho) * gm1;
-  const double pS = (Us == 0.0 && Ur > 0.0) ? Us : Us * pow(Ur, gm1);
+  double pS = 0.0;
+  if constexpr (PSL) {  // entropy S = p_S / rho^(gamma-1), updated and back
+    const double ps0 = W[x + 5 * fs];
+    const double S0 = (ps0 == 0.0 && r0 > 0.0) ? ps0 : ps0 / pow(r0, gm1);
+    const double Us = S0 - dt * (double)du[5];
+    pS = (Us == 0.0 && Ur > 0.0) ? Us : Us * pow(Ur, gm1);
+  }
   // positivity floors (src/solver_func.c:2117-2135)
   if (rho < P.rho_floor) {
     rho = P.rho_floor;
@@ -665,7 +671,7 @@ __device__ __forceinline__ void update_cart(const Params& P, const Work<R>& wk, 
   Wn[x + 2 * fs] = vv[1];
   Wn[x + 3 * fs] = vv[2];
   Wn[x + 4 * fs] = p;
-  Wn[x + 5 * fs] = pS;
+  if constexpr (PSL) Wn[x + 5 * fs] = pS;  // else it stays zero in both buffers
 
   // CFL dt of the new state with magtot = mags^{n+1} (src/solver_func.c:255-298)
   {
@@ -684,11 +690,11 @@ __device__ __forceinline__ void update_cart(const Params& P, const Work<R>& wk, 
 }
 
 // one active cell: returns its CFL dt and |div B| of the new state
-template <int COORD, typename R, bool BG>
+template <int COORD, typename R, bool BG, bool PSL>
 __device__ __forceinline__ void update_body(const Params& P, const Work<R>& wk, Pos t,
                                             double& dtc, double& dbmax) {
   if constexpr (COORD == 0) {
-    update_cart<R, BG>(P, wk, t, dtc, dbmax);
+    update_cart<R, BG, PSL>(P, wk, t, dtc, dbmax);
     return;
   }
   const int i = NGH + t.x, j = NGH + t.y, k = NGH + t.z;
@@ -715,6 +721,7 @@ __device__ __forceinline__ void update_body(const Params& P, const Work<R>& wk, 
     const R* Fd = F + (size_t)(9 * d) * fs + x;
 #pragma unroll
     for (int m = 0; m < 6; m++) {
+      if (m == PS && !PSL) continue;
       double v = ((double)Fd[s + m * fs] * fu[d] - (double)Fd[m * fs] * fl[d]) * ivol;
       du[m] = d == 0 ? v : du[m] + v;
     }
@@ -788,26 +795,33 @@ __device__ __forceinline__ void update_body(const Params& P, const Work<R>& wk, 
   // U^n from W^n (src/solver_func.c:356-382)
   const double gm1 = P.gm1;
   const double r0 = W[x], u0 = W[x + fs], v0 = W[x + 2 * fs], w0 = W[x + 3 * fs],
-               p0 = W[x + 4 * fs], ps0 = W[x + 5 * fs];
+               p0 = W[x + 4 * fs];
   double U[6];
   U[0] = r0;
   U[1] = r0 * u0;
   U[2] = r0 * v0;
   U[3] = r0 * w0;
   U[4] = 0.5 * r0 * (u0 * u0 + v0 * v0 + w0 * w0) + p0 * P.inv_gm1;
-  U[5] = (ps0 == 0.0 && r0 > 0.0) ? ps0 : ps0 / pow(r0, gm1);
+  U[5] = 0.0;
+  if constexpr (PSL) {
+    const double ps0 = W[x + 5 * fs];
+    U[5] = (ps0 == 0.0 && r0 > 0.0) ? ps0 : ps0 / pow(r0, gm1);
+  }
   const double U0[3] = {U[1], U[2], U[3]};
   // conservative update and cons->prim (src/solver_solve.c:326-377)
   U[0] -= dt * du[0];
 #pragma unroll
   for (int a = 0; a < 3; a++) U[1 + a] = U[1 + a] - dt * du[1 + a] + dt * sh[a];
   U[4] -= dt * du[4];
-  U[5] -= dt * du[5];
   double rho = U[0];
   const double irho = 1.0 / U[0];
   double vv[3] = {U[1] * irho, U[2] * irho, U[3] * irho};
   double p = (U[4] - 0.5 * (vv[0] * vv[0] + vv[1] * vv[1] + vv[2] * vv[2]) * rho) * gm1;
-  const double pS = (U[5] == 0.0 && U[0] > 0.0) ? U[5] : U[5] * pow(U[0], gm1);
+  double pS = 0.0;
+  if constexpr (PSL) {
+    U[5] -= dt * du[5];
+    pS = (U[5] == 0.0 && U[0] > 0.0) ? U[5] : U[5] * pow(U[0], gm1);
+  }
   // positivity floors (src/solver_func.c:2117-2135)
   if (rho < P.rho_floor) {
     rho = P.rho_floor;
@@ -849,7 +863,7 @@ __device__ __forceinline__ void update_body(const Params& P, const Work<R>& wk, 
   Wn[x + 2 * fs] = vv[1];
   Wn[x + 3 * fs] = vv[2];
   Wn[x + 4 * fs] = p;
-  Wn[x + 5 * fs] = pS;
+  if constexpr (PSL) Wn[x + 5 * fs] = pS;
   // CFL dt of the new state (magtot = mags^{n+1}) and max|div B^{n+1}|
   dtc = cfl_cell<COORD>(P, i, j, k, rho, vv[0], vv[1], vv[2], p, mn[0], mn[1], mn[2]);
   double b0l[3] = {0.0, 0.0, 0.0}, b0u[3] = {0.0, 0.0, 0.0};
@@ -929,6 +943,7 @@ __device__ __forceinline__ void wrap_body(const Params& P, int axis, int which, 
   const int N = P.N[axis];
   const int side = lay / NGH, l = lay % NGH;
   for (int f = 0; f < 9; f++) {
+    if (f == PS && !P.ps_live) continue;  // zero everywhere, and stays so
     const int onface = (f >= 6 && f - 6 == axis) ? 1 : 0;
     double* a = f < 6 ? W + (size_t)f * P.fs : B + (size_t)(f - 6) * P.fs;
     int src, dst;
@@ -961,6 +976,7 @@ __device__ __forceinline__ void bcface_body(const Params& P, int axis, int side,
   double* __restrict__ B = P.Bbuf[bsel];
   const int N = P.N[axis];
   for (int f = 0; f < 9; f++) {
+    if (f == PS && !P.ps_live) continue;  // zero everywhere, and stays so
     const bool gas = f < 6;
     const int kd = gas ? kind : gkind;
     if (kd == 0 || kd == 'n' || kd == 'p') continue;
@@ -1028,7 +1044,7 @@ __device__ __forceinline__ void bcface_body(const Params& P, int axis, int side,
 #define GOP_MINB_FLUX_F32 4
 #endif
 #ifndef GOP_MINB_UPDATE_F64
-#define GOP_MINB_UPDATE_F64 3
+#define GOP_MINB_UPDATE_F64 2
 #endif
 #ifndef GOP_MINB_UPDATE_F32
 #define GOP_MINB_UPDATE_F32 4
@@ -1107,10 +1123,10 @@ __global__ void k_ring_dt(Params P) {
   block_commit(dtc, db, P.scal + S_NEXT_DT, P.scal + S_DIVB);
 }
 
-template <typename R>
+template <typename R, bool PSL>
 __global__ void __launch_bounds__(256, GOP_MINB(AB2, R)) k_ab2(Params P, Work<R> w) {
   if (stopped(P)) return;
-  ab2_body<R>(P, w, grid_pos());
+  ab2_body<R, PSL>(P, w, grid_pos());
 }
 template <typename R, int D>
 __global__ void __launch_bounds__(256, GOP_MINB(C2C, R)) k_c2c(Params P, Work<R> w) {
@@ -1128,11 +1144,11 @@ __global__ void __launch_bounds__(256, GOP_MINB(FLUX, R)) k_flux(Params P, Work<
   if (stopped(P)) return;
   flux_body<R, D, BG, PSL>(P, w, grid_pos());
 }
-template <int COORD, typename R, bool BG>
+template <int COORD, typename R, bool BG, bool PSL>
 __global__ void __launch_bounds__(256, GOP_UPD_MINB(COORD, R)) k_update(Params P, Work<R> w) {
   if (stopped(P)) return;
   double dtc = DBL_MAX, db = 0.0;
-  update_body<COORD, R, BG>(P, w, grid_pos(), dtc, db);
+  update_body<COORD, R, BG, PSL>(P, w, grid_pos(), dtc, db);
   block_commit(dtc, db, P.scal + S_NEXT_DT, P.scal + S_DIVB);
 }
 __global__ void k_wrap(Params P, int axis, int which) {
@@ -1272,7 +1288,10 @@ static void launch_slot_bg(const Params& P, int coord, const Work<R>& w, int slo
   const dim3 sp = launch_space(P, slot);
   const dim3 g = grid3(sp.x, sp.y, sp.z, blk);
   switch (slot) {
-    case K_AB2: LAUNCH(k_ab2<R>, g, blk, st, P, w); break;
+    case K_AB2:
+      if (P.ps_live) LAUNCH((k_ab2<R, true>), g, blk, st, P, w);
+      else LAUNCH((k_ab2<R, false>), g, blk, st, P, w);
+      break;
     case K_C2C0: LAUNCH((k_c2c<R, 0>), g, blk, st, P, w); break;
     case K_C2C1: LAUNCH((k_c2c<R, 1>), g, blk, st, P, w); break;
     case K_C2C2: LAUNCH((k_c2c<R, 2>), g, blk, st, P, w); break;
@@ -1292,8 +1311,13 @@ static void launch_slot_bg(const Params& P, int coord, const Work<R>& w, int slo
       else LAUNCH((k_flux<R, 2, BG, false>), g, blk, st, P, w);
       break;
     case K_UPDATE:
-      if (coord == 0) LAUNCH((k_update<0, R, BG>), g, blk, st, P, w);
-      else LAUNCH((k_update<2, R, BG>), g, blk, st, P, w);
+      if (coord == 0) {
+        if (P.ps_live) LAUNCH((k_update<0, R, BG, true>), g, blk, st, P, w);
+        else LAUNCH((k_update<0, R, BG, false>), g, blk, st, P, w);
+      } else {
+        if (P.ps_live) LAUNCH((k_update<2, R, BG, true>), g, blk, st, P, w);
+        else LAUNCH((k_update<2, R, BG, false>), g, blk, st, P, w);
+      }
       break;
     default: break;
   }
