@@ -3,11 +3,12 @@
 GAMERA-OP carries p_S = S rho^(gamma-1) through the step with its own
 Rusanov flux (VF_entropy, src/solver_func.c:940-1033) and the
 conservative update of S (src/solver_solve.c:326-377); every supplied
-problem leaves it at zero.  The CUDA flux kernels skip the reconstruction
-of p_S while it is identically zero on the grid (a device flag that the AB2
-stage sets from the state it reads), so these cases, with p_S = f * p from
-GOP_PS in the oracle's problem file, check the live channel against the
-reference binary and that the skip changes nothing.
+problem leaves it at zero.  gop_prepare checks p_S of the state and its
+AB2 history; while it is identically zero (then it stays zero) the step
+runs kernel variants that leave the channel out.  These cases, with
+p_S = f * p from GOP_PS in the oracle's problem file, check the live
+channel against the reference binary and the C restatement, and that a
+batch picks up a member whose channel turns live.
 """
 import math
 
