@@ -689,6 +689,47 @@ __device__ __forceinline__ void update_cart(const Params& P, const Work<R>& wk, 
     P.scal[S_FLAGS] = 1.0;
 }
 
+// Constrained transport of a curvilinear grid (src/solver_solve.c:263-306),
+// its own launch before the update: every active cell writes its three lower
+// faces, the last cell along an axis also the upper boundary face, so each
+// face (with its division by the face area) is computed once
+template <int COORD, typename R>
+__device__ __forceinline__ void ct_body(const Params& P, const Work<R>& wk, Pos t) {
+  const int i = NGH + t.x, j = NGH + t.y, k = NGH + t.z;
+  if (i >= NGH + P.n[0] || j >= NGH + P.n[1] || k >= NGH + P.n[2]) return;
+  const size_t fs = P.fs;
+  const double dt = P.scal[S_DT];
+  const int cb = cur_buf(P);
+  const double* __restrict__ B = P.Bbuf[cb];
+  double* __restrict__ Bn = P.Bbuf[1 - cb];
+  const R* __restrict__ E = wk.E;
+  const long long x = lin(P, i, j, k);
+  const bool last[3] = {i == NGH + P.n[0] - 1, j == NGH + P.n[1] - 1, k == NGH + P.n[2] - 1};
+  double bl[3], bu[3] = {0.0, 0.0, 0.0};
+  bl[0] = ct_face<COORD, 0, R>(P, B, E, i, j, k, dt);
+  bl[1] = ct_face<COORD, 1, R>(P, B, E, i, j, k, dt);
+  bl[2] = ct_face<COORD, 2, R>(P, B, E, i, j, k, dt);
+  if (last[0]) bu[0] = ct_face<COORD, 0, R>(P, B, E, i + 1, j, k, dt);
+  if (last[1]) bu[1] = ct_face<COORD, 1, R>(P, B, E, i, j + 1, k, dt);
+  if (last[2]) bu[2] = ct_face<COORD, 2, R>(P, B, E, i, j, k + 1, dt);
+  if (COORD == 2 && P.ring) {
+    // B_j on a pole face (zero area) from the face next to it and the one
+    // half a turn away in phi (tackle_Magfield_pole,
+    // spherical_RingAverage.c:205-233)
+    const int ko = NGH + (k - NGH + P.n[2] / 2) % P.n[2];
+    if ((P.ring & 1) && j == NGH)
+      bl[1] = 0.5 * (ct_face<COORD, 1, R>(P, B, E, i, j + 1, k, dt) -
+                     ct_face<COORD, 1, R>(P, B, E, i, j + 1, ko, dt));
+    if ((P.ring & 2) && last[1])
+      bu[1] = 0.5 * (bl[1] - ct_face<COORD, 1, R>(P, B, E, i, j, ko, dt));
+  }
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    Bn[x + a * fs] = bl[a];
+    if (last[a]) Bn[x + stride(P, a) + a * fs] = bu[a];
+  }
+}
+
 // one active cell: returns its CFL dt and |div B| of the new state
 template <int COORD, typename R, bool BG, bool PSL>
 __device__ __forceinline__ void update_body(const Params& P, const Work<R>& wk, Pos t,
@@ -707,7 +748,6 @@ __device__ __forceinline__ void update_body(const Params& P, const Work<R>& wk, 
   double* __restrict__ Wn = P.Wbuf[1 - cb];
   double* __restrict__ Bn = P.Bbuf[1 - cb];
   const R* __restrict__ F = wk.F;
-  const R* __restrict__ E = wk.E;
   const long long x = lin(P, i, j, k);
   const double vol = Geo<COORD>::vol(P, i, j, k);
   const double ivol = 1.0 / vol;
@@ -768,29 +808,13 @@ __device__ __forceinline__ void update_body(const Params& P, const Work<R>& wk, 
     sb[2] = -((double)Fi[8 * fs] * fi0 + (double)Fi[si + 8 * fs] * fi1) * geo;
     sb[2] += -((double)Fj[8 * fs] * fj0 + (double)Fj[sjj + 8 * fs] * fj1) * sr;
   }
-  // new face fields: this cell's lower faces and its upper faces
+  // the new face fields of this cell's lower and upper faces, written by
+  // k_ct before this launch
   double bl[3], bu[3];
-  bl[0] = ct_face<COORD, 0, R>(P, B, E, i, j, k, dt);
-  bl[1] = ct_face<COORD, 1, R>(P, B, E, i, j, k, dt);
-  bl[2] = ct_face<COORD, 2, R>(P, B, E, i, j, k, dt);
-  bu[0] = ct_face<COORD, 0, R>(P, B, E, i + 1, j, k, dt);
-  bu[1] = ct_face<COORD, 1, R>(P, B, E, i, j + 1, k, dt);
-  bu[2] = ct_face<COORD, 2, R>(P, B, E, i, j, k + 1, dt);
-  if (COORD == 2 && P.ring) {
-    // B_j on a pole face (zero area) from the face next to it and the one
-    // half a turn away in phi (tackle_Magfield_pole,
-    // spherical_RingAverage.c:205-233)
-    const int ko = NGH + (k - NGH + P.n[2] / 2) % P.n[2];
-    if ((P.ring & 1) && j == NGH)
-      bl[1] = 0.5 * (bu[1] - ct_face<COORD, 1, R>(P, B, E, i, j + 1, ko, dt));
-    if ((P.ring & 2) && j == NGH + P.n[1] - 1)
-      bu[1] = 0.5 * (bl[1] - ct_face<COORD, 1, R>(P, B, E, i, j, ko, dt));
-  }
 #pragma unroll
   for (int a = 0; a < 3; a++) {
-    Bn[x + a * fs] = bl[a];
-    const int pos = a == 0 ? i : (a == 1 ? j : k);
-    if (pos == NGH + P.n[a] - 1) Bn[x + stride(P, a) + a * fs] = bu[a];
+    bl[a] = Bn[x + a * fs];
+    bu[a] = Bn[x + stride(P, a) + a * fs];
   }
   // U^n from W^n (src/solver_func.c:356-382)
   const double gm1 = P.gm1;
@@ -1052,6 +1076,9 @@ __device__ __forceinline__ void bcface_body(const Params& P, int axis, int side,
 #ifndef GOP_MINB_UPDATE_SPH
 #define GOP_MINB_UPDATE_SPH 2
 #endif
+#ifndef GOP_MINB_CT
+#define GOP_MINB_CT 4
+#endif
 #define GOP_MINB(STAGE, R) (sizeof(R) == 8 ? GOP_MINB_##STAGE##_F64 : GOP_MINB_##STAGE##_F32)
 #define GOP_UPD_MINB(COORD, R) ((COORD) == 0 ? GOP_MINB(UPDATE, R) : GOP_MINB_UPDATE_SPH)
 
@@ -1143,6 +1170,11 @@ template <typename R, int D, bool BG, bool PSL>
 __global__ void __launch_bounds__(256, GOP_MINB(FLUX, R)) k_flux(Params P, Work<R> w) {
   if (stopped(P)) return;
   flux_body<R, D, BG, PSL>(P, w, grid_pos());
+}
+template <int COORD, typename R>
+__global__ void __launch_bounds__(256, GOP_MINB_CT) k_ct(Params P, Work<R> w) {
+  if (stopped(P)) return;
+  ct_body<COORD, R>(P, w, grid_pos());
 }
 template <int COORD, typename R, bool BG, bool PSL>
 __global__ void __launch_bounds__(256, GOP_UPD_MINB(COORD, R)) k_update(Params P, Work<R> w) {
@@ -1351,6 +1383,10 @@ void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t
   }
   hook(G_UPDATE, 1);
   launch_pole_emf<R>(P, w, st);  // pole ring average only
+  if (coord != 0) {  // curvilinear: the face fields in their own launch
+    const dim3 blk = tune.blk[K_UPDATE];
+    LAUNCH((k_ct<2, R>), grid3(P.n[0], P.n[1], P.n[2], blk), blk, st, P, w);
+  }
   launch_slot<R>(P, coord, w, K_UPDATE, tune.blk[K_UPDATE], st);
   // the work arrays are free after the update: 2 fields of doubles of scratch
   if (P.ring) {
