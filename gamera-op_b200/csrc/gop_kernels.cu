@@ -82,23 +82,25 @@ __device__ __forceinline__ void block_commit(double a, double b, double* smin, d
   }
 }
 
-// CFL time step of one cell (src/solver_func.c:255-298)
-template <int COORD>
+// CFL time step of one cell (src/solver_func.c:255-298), in T arithmetic
+// (FP32 for the mixed path's estimate)
+template <int COORD, typename T = double>
 __device__ __forceinline__ double cfl_cell(const Params& P, int i, int j, int k, double rho,
                                            double u, double v, double w, double p, double b1,
                                            double b2, double b3) {
-  double bsq = b1 * b1 + b2 * b2 + b3 * b3;
-  double va = sqrt(bsq / rho);
-  double vae = va * P.ca / sqrt(va * va + P.ca2);
-  double vf = sqrt(u * u + v * v + w * w);
-  double vs = sqrt(P.gamma * p / rho);
-  double vc = vf + sqrt(vs * vs + vae * vae);
-  double dk = Geo<COORD>::dl(P, 2, i, j, k);
+  const T r = (T)rho, x1 = (T)b1, x2 = (T)b2, x3 = (T)b3, ut = (T)u, vt = (T)v, wt = (T)w;
+  T bsq = x1 * x1 + x2 * x2 + x3 * x3;
+  T va = sqrt(bsq / r);
+  T vae = va * (T)P.ca / sqrt(va * va + (T)P.ca2);
+  T vf = sqrt(ut * ut + vt * vt + wt * wt);
+  T vs = sqrt((T)P.gamma * (T)p / r);
+  T vc = vf + sqrt(vs * vs + vae * vae);
+  T dk = (T)Geo<COORD>::dl(P, 2, i, j, k);
   // the phi length of the pole rings is nk / nchunk times longer (dxk_ring,
   // spherical_RingAverage.c:110-138; get_dt_ring, spherical_general.c:700-743)
-  if (COORD == 2 && P.ring) dk = P.ringtab[2 * P.n[2] + j] * dk;
-  double t = vc / Geo<COORD>::dl(P, 0, i, j, k) + vc / Geo<COORD>::dl(P, 1, i, j, k) + vc / dk;
-  return P.cfl / t;
+  if (COORD == 2 && P.ring) dk = (T)P.ringtab[2 * P.n[2] + j] * dk;
+  T t = vc / (T)Geo<COORD>::dl(P, 0, i, j, k) + vc / (T)Geo<COORD>::dl(P, 1, i, j, k) + vc / dk;
+  return (double)((T)P.cfl / t);
 }
 
 // rows of cells whose state or face field the pole ring average changes
@@ -730,7 +732,10 @@ __device__ __forceinline__ void ct_body(const Params& P, const Work<R>& wk, Pos 
   }
 }
 
-// one active cell: returns its CFL dt and |div B| of the new state
+// one active cell: returns its CFL dt and |div B| of the new state.  The
+// flux divergence, the geometric sources, the Alfven/Boris correction and
+// the CFL estimate are in R (FP32 on the mixed path); the face fields, the
+// conservative update and the pressure recovery are FP64.
 template <int COORD, typename R, bool BG, bool PSL>
 __device__ __forceinline__ void update_body(const Params& P, const Work<R>& wk, Pos t,
                                             double& dtc, double& dbmax) {
@@ -751,7 +756,9 @@ __device__ __forceinline__ void update_body(const Params& P, const Work<R>& wk, 
   const long long x = lin(P, i, j, k);
   const double vol = Geo<COORD>::vol(P, i, j, k);
   const double ivol = 1.0 / vol;
-  double du[6], dm[3], fl[3], fu[3];
+  const R rivol = (R)ivol;
+  R du[6], dm[3];
+  double fl[3], fu[3];
 #pragma unroll
   for (int d = 0; d < 3; d++) {
     const long long s = stride(P, d);
@@ -762,51 +769,51 @@ __device__ __forceinline__ void update_body(const Params& P, const Work<R>& wk, 
 #pragma unroll
     for (int m = 0; m < 6; m++) {
       if (m == PS && !PSL) continue;
-      double v = ((double)Fd[s + m * fs] * fu[d] - (double)Fd[m * fs] * fl[d]) * ivol;
+      const R v = ((R)Fd[s + m * fs] * (R)fu[d] - (R)Fd[m * fs] * (R)fl[d]) * rivol;
       du[m] = d == 0 ? v : du[m] + v;
     }
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-      double v = ((double)Fd[s + (6 + a) * fs] * fu[d] - (double)Fd[(6 + a) * fs] * fl[d]) * ivol;
+      const R v = ((R)Fd[s + (6 + a) * fs] * (R)fu[d] - (R)Fd[(6 + a) * fs] * (R)fl[d]) * rivol;
       dm[a] = d == 0 ? v : dm[a] + v;
     }
   }
   if constexpr (BG) {  // + the Lorentz force of B0 (src/solver_solve.c:312-324)
 #pragma unroll
-    for (int a = 0; a < 3; a++) dm[a] += P.bg[(size_t)(BG_LOR + a) * fs + x];
+    for (int a = 0; a < 3; a++) dm[a] += (R)P.bg[(size_t)(BG_LOR + a) * fs + x];
   }
   // spherical geometric sources (src/spherical/spherical_general.c:605-681)
-  double sh[3] = {0.0, 0.0, 0.0}, sb[3] = {0.0, 0.0, 0.0};
+  R sh[3] = {R(0), R(0), R(0)}, sb[3] = {R(0), R(0), R(0)};
   if (COORD == 2) {
     const long long si = 1, sjj = P.sj;
-    const double fi0 = fl[0], fi1 = fu[0], fj0 = fl[1], fj1 = fu[1];
-    const double dr = tb(P, 0, T_DX, i), rc = tb(P, 0, T_G3, i);
+    const R fi0 = (R)fl[0], fi1 = (R)fu[0], fj0 = (R)fl[1], fj1 = (R)fu[1];
+    const R dr = (R)tb(P, 0, T_DX, i), rc = (R)tb(P, 0, T_G3, i);
     const R* Wh = wk.Wh + x;
-    const double ph = Wh[PR * fs], rh = Wh[RHO * fs], v2h = Wh[V2 * fs], v3h = Wh[V3 * fs];
-    const double m22 = ph + rh * v2h * v2h, m33 = ph + rh * v3h * v3h;
+    const R ph = (R)Wh[PR * fs], rh = (R)Wh[RHO * fs], v2h = (R)Wh[V2 * fs], v3h = (R)Wh[V3 * fs];
+    const R m22 = ph + rh * v2h * v2h, m33 = ph + rh * v3h * v3h;
     const R* Fi = F + x;
     const R* Fj = F + (size_t)9 * fs + x;
-    const double geo = dr / rc / 2.0 * ivol;
-    sh[0] = 0.5 * (m22 + m33) * (fi1 - fi0) * ivol;
-    sh[1] = -((double)Fi[2 * fs] * fi0 + (double)Fi[si + 2 * fs] * fi1) * geo + (fj1 - fj0) * ivol * m33;
-    sh[2] = -((double)Fi[3 * fs] * fi0 + (double)Fi[si + 3 * fs] * fi1) * geo;
-    const double sr = tb(P, 1, T_G3, j) / tb(P, 1, T_G4, j) * ivol;
-    sh[2] += -((double)Fj[3 * fs] * fj0 + (double)Fj[sjj + 3 * fs] * fj1) * sr;
+    const R geo = dr / rc / R(2) * rivol;
+    sh[0] = R(0.5) * (m22 + m33) * (fi1 - fi0) * rivol;
+    sh[1] = -((R)Fi[2 * fs] * fi0 + (R)Fi[si + 2 * fs] * fi1) * geo + (fj1 - fj0) * rivol * m33;
+    sh[2] = -((R)Fi[3 * fs] * fi0 + (R)Fi[si + 3 * fs] * fi1) * geo;
+    const R sr = (R)tb(P, 1, T_G3, j) / (R)tb(P, 1, T_G4, j) * rivol;
+    sh[2] += -((R)Fj[3 * fs] * fj0 + (R)Fj[sjj + 3 * fs] * fj1) * sr;
     const R* Msh = wk.Msh + x;
-    const double b1 = Msh[0], b2 = Msh[fs], b3 = Msh[2 * fs];
-    double bsq = b1 * b1 + b2 * b2 + b3 * b3;
-    double n22 = 0.5 * bsq - b2 * b2, n33 = 0.5 * bsq - b3 * b3;
+    const R b1 = (R)Msh[0], b2 = (R)Msh[fs], b3 = (R)Msh[2 * fs];
+    R bsq = b1 * b1 + b2 * b2 + b3 * b3;
+    R n22 = R(0.5) * bsq - b2 * b2, n33 = R(0.5) * bsq - b3 * b3;
     if constexpr (BG) {  // with the B0 cross terms (spherical_general.c:634-638)
       const double* c0 = P.bg + (size_t)BG_B0 * fs + x;
-      const double g1 = c0[0], g2 = c0[fs], g3 = c0[2 * fs];
-      bsq = b1 * b1 + b2 * b2 + b3 * b3 + 2 * (b1 * g1 + b2 * g2 + b3 * g3);
-      n22 = 0.5 * bsq - (b2 + g2) * b2 - b2 * g2;
-      n33 = 0.5 * bsq - (b3 + g3) * b3 - b3 * g3;
+      const R g1 = (R)c0[0], g2 = (R)c0[fs], g3 = (R)c0[2 * fs];
+      bsq = b1 * b1 + b2 * b2 + b3 * b3 + R(2) * (b1 * g1 + b2 * g2 + b3 * g3);
+      n22 = R(0.5) * bsq - (b2 + g2) * b2 - b2 * g2;
+      n33 = R(0.5) * bsq - (b3 + g3) * b3 - b3 * g3;
     }
-    sb[0] = 0.5 * (n22 + n33) * (fi1 - fi0) * ivol;
-    sb[1] = -((double)Fi[7 * fs] * fi0 + (double)Fi[si + 7 * fs] * fi1) * geo + (fj1 - fj0) * ivol * n33;
-    sb[2] = -((double)Fi[8 * fs] * fi0 + (double)Fi[si + 8 * fs] * fi1) * geo;
-    sb[2] += -((double)Fj[8 * fs] * fj0 + (double)Fj[sjj + 8 * fs] * fj1) * sr;
+    sb[0] = R(0.5) * (n22 + n33) * (fi1 - fi0) * rivol;
+    sb[1] = -((R)Fi[7 * fs] * fi0 + (R)Fi[si + 7 * fs] * fi1) * geo + (fj1 - fj0) * rivol * n33;
+    sb[2] = -((R)Fi[8 * fs] * fi0 + (R)Fi[si + 8 * fs] * fi1) * geo;
+    sb[2] += -((R)Fj[8 * fs] * fj0 + (R)Fj[sjj + 8 * fs] * fj1) * sr;
   }
   // the new face fields of this cell's lower and upper faces, written by
   // k_ct before this launch
@@ -833,17 +840,17 @@ __device__ __forceinline__ void update_body(const Params& P, const Work<R>& wk, 
   }
   const double U0[3] = {U[1], U[2], U[3]};
   // conservative update and cons->prim (src/solver_solve.c:326-377)
-  U[0] -= dt * du[0];
+  U[0] -= dt * (double)du[0];
 #pragma unroll
-  for (int a = 0; a < 3; a++) U[1 + a] = U[1 + a] - dt * du[1 + a] + dt * sh[a];
-  U[4] -= dt * du[4];
+  for (int a = 0; a < 3; a++) U[1 + a] = U[1 + a] - dt * (double)du[1 + a] + dt * (double)sh[a];
+  U[4] -= dt * (double)du[4];
   double rho = U[0];
   const double irho = 1.0 / U[0];
   double vv[3] = {U[1] * irho, U[2] * irho, U[3] * irho};
   double p = (U[4] - 0.5 * (vv[0] * vv[0] + vv[1] * vv[1] + vv[2] * vv[2]) * rho) * gm1;
   double pS = 0.0;
   if constexpr (PSL) {
-    U[5] -= dt * du[5];
+    U[5] -= dt * (double)du[5];
     pS = (U[5] == 0.0 && U[0] > 0.0) ? U[5] : U[5] * pow(U[0], gm1);
   }
   // positivity floors (src/solver_func.c:2117-2135)
@@ -866,21 +873,26 @@ __device__ __forceinline__ void update_body(const Params& P, const Work<R>& wk, 
       mn[a] += c0;  // the next step's magtot, for its CFL dt
     }
   }
-  const double bsq = mt[0] * mt[0] + mt[1] * mt[1] + mt[2] * mt[2];
-  const double alf = bsq / rho / P.ca2;
-  const double perp = 1.0 / (1.0 + alf);
-  const double drho = -dt * du[0];
-  const double dva = alf * drho;
-  double tv[3];
-#pragma unroll
-  for (int a = 0; a < 3; a++) tv[a] = alf * (-dt * du[1 + a] + dt * sh[a] - drho * W[x + (1 + a) * fs]);
-  double bdv = mt[0] * tv[0] + mt[1] * tv[1] + mt[2] * tv[2];
-  bdv = bdv / (bsq + 1e-10);
+  const R mr[3] = {(R)mt[0], (R)mt[1], (R)mt[2]};
+  const R bsq = mr[0] * mr[0] + mr[1] * mr[1] + mr[2] * mr[2];
+  const R alf = bsq / (R)rho / (R)P.ca2;
+  const R perp = R(1) / (R(1) + alf);
+  const R rdt = (R)dt;
+  const R drho = -rdt * du[0];
+  const R dva = alf * drho;
+  R tv[3], wv[3];
 #pragma unroll
   for (int a = 0; a < 3; a++) {
-    const double mom = U0[a] + perp * ((-dt * du[1 + a] + dt * sh[a]) + (-dt * dm[a] + dt * sb[a]) +
-                                       dva * W[x + (1 + a) * fs] + mt[a] * bdv);
-    vv[a] = mom * irho;
+    wv[a] = (R)W[x + (1 + a) * fs];
+    tv[a] = alf * (-rdt * du[1 + a] + rdt * sh[a] - drho * wv[a]);
+  }
+  R bdv = mr[0] * tv[0] + mr[1] * tv[1] + mr[2] * tv[2];
+  bdv = bdv / (bsq + R(1e-10));
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const R inc = perp * ((-rdt * du[1 + a] + rdt * sh[a]) + (-rdt * dm[a] + rdt * sb[a]) +
+                          dva * wv[a] + mr[a] * bdv);
+    vv[a] = (U0[a] + (double)inc) * irho;
   }
   Wn[x] = rho;
   Wn[x + fs] = vv[0];
@@ -889,7 +901,7 @@ __device__ __forceinline__ void update_body(const Params& P, const Work<R>& wk, 
   Wn[x + 4 * fs] = p;
   if constexpr (PSL) Wn[x + 5 * fs] = pS;
   // CFL dt of the new state (magtot = mags^{n+1}) and max|div B^{n+1}|
-  dtc = cfl_cell<COORD>(P, i, j, k, rho, vv[0], vv[1], vv[2], p, mn[0], mn[1], mn[2]);
+  dtc = cfl_cell<COORD, R>(P, i, j, k, rho, vv[0], vv[1], vv[2], p, mn[0], mn[1], mn[2]);
   double b0l[3] = {0.0, 0.0, 0.0}, b0u[3] = {0.0, 0.0, 0.0};
   if constexpr (BG) {  // div of B + B0 (face-normal B0, src/solver_func.c:324-343)
 #pragma unroll
@@ -1073,14 +1085,17 @@ __device__ __forceinline__ void bcface_body(const Params& P, int axis, int side,
 #ifndef GOP_MINB_UPDATE_F32
 #define GOP_MINB_UPDATE_F32 4
 #endif
-#ifndef GOP_MINB_UPDATE_SPH
-#define GOP_MINB_UPDATE_SPH 2
+#ifndef GOP_MINB_UPDATE_SPH_F64
+#define GOP_MINB_UPDATE_SPH_F64 2
+#endif
+#ifndef GOP_MINB_UPDATE_SPH_F32
+#define GOP_MINB_UPDATE_SPH_F32 2
 #endif
 #ifndef GOP_MINB_CT
 #define GOP_MINB_CT 4
 #endif
 #define GOP_MINB(STAGE, R) (sizeof(R) == 8 ? GOP_MINB_##STAGE##_F64 : GOP_MINB_##STAGE##_F32)
-#define GOP_UPD_MINB(COORD, R) ((COORD) == 0 ? GOP_MINB(UPDATE, R) : GOP_MINB_UPDATE_SPH)
+#define GOP_UPD_MINB(COORD, R) ((COORD) == 0 ? GOP_MINB(UPDATE, R) : GOP_MINB(UPDATE_SPH, R))
 
 __global__ void k_begin(Params P) { begin_body(P); }
 __global__ void k_end(Params P) { end_body(P); }
