@@ -51,24 +51,27 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def algorithmic_bytes(group, n, mixed=False):
+def algorithmic_bytes(group, n, mixed=False, ps_live=False):
     """Compulsory DRAM bytes of one launch of a kernel group (each input
     array element read once, each output written once).  Work arrays are
-    FP32 on the mixed path (4 bytes), the state and its AB2 history FP64."""
+    FP32 on the mixed path (4 bytes), the state and its AB2 history FP64.
+    ps_live False: the entropy channel p_S is identically zero (every
+    problem measured here), and the step's kernels leave it out."""
     ni, nj, nk = n
     cells = ni * nj * nk
     ext = (ni + 9) * (nj + 9) * (nk + 9)
     w = 4 if mixed else 8  # element size of the work arrays
-    if group == "flux":   # per direction: Wh 6, W 6, mags_h 3, mags 3, B_n 1 in; 9 fluxes, 2 edge velocities out
-        return 30 * w * (cells + nj * nk)
+    g = 6 if ps_live else 5  # gas fields the step moves
+    if group == "flux":   # per direction: Wh g, W g, mags_h 3, mags 3, B_n 1 in; g+3 fluxes, 2 edge velocities out
+        return (3 * g + 12) * w * (cells + nj * nk)
     if group == "emf":    # per direction: 2 velocities, 2 B_h, 2 B, rho_h in; E out
         return 8 * w * cells
     if group == "c2c":    # per direction: 2 W_h, 2 W in; 2 edge velocities out (ghost layers)
         return 6 * w * (ni + 1) * 8 * nk
-    if group == "update":  # W 6, B 3 in and out (FP64); 27 fluxes, 3 EMFs in
-        return (18 * 8 + 30 * w) * cells
+    if group == "update":  # W g, B 3 in and out (FP64); 3 (g+3) fluxes, 3 EMFs in
+        return (2 * (g + 3) * 8 + (3 * (g + 3) + 3) * w) * cells
     if group == "ab2":    # W, W_old, B, B_old in (FP64); W_h, mags, mags_h, B_h out (+ W, B copies when mixed)
-        return (18 * 8 + (15 + (9 if mixed else 0)) * w) * ext
+        return (2 * (g + 3) * 8 + (g + 9 + ((g + 3) if mixed else 0)) * w) * ext
     return 0
 
 
