@@ -38,6 +38,16 @@ enum { RHO = 0, V1, V2, V3, PR, PS };
 
 __device__ __forceinline__ bool stopped(const Params& P) { return P.scal[S_STOP] != 0.0; }
 
+// Programmatic dependent launch: LAUNCH lets each kernel start launching
+// while its predecessor on the stream is still running.  Every kernel it
+// launches first waits here until that predecessor has completed and its
+// writes are visible, then lets its own successor start launching, so only
+// launch latency and block scheduling overlap, never the work.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 __device__ __forceinline__ void atomic_min_pos(double* slot, double v) {
   // positive doubles order like their bit patterns
   atomicMin(reinterpret_cast<unsigned long long*>(slot), (unsigned long long)__double_as_longlong(v));
@@ -1097,13 +1107,23 @@ __device__ __forceinline__ void bcface_body(const Params& P, int axis, int side,
 #define GOP_MINB(STAGE, R) (sizeof(R) == 8 ? GOP_MINB_##STAGE##_F64 : GOP_MINB_##STAGE##_F32)
 #define GOP_UPD_MINB(COORD, R) ((COORD) == 0 ? GOP_MINB(UPDATE, R) : GOP_MINB(UPDATE_SPH, R))
 
-__global__ void k_begin(Params P) { begin_body(P); }
-__global__ void k_end(Params P) { end_body(P); }
-__global__ void k_arm(Params P, double tstop, double budget) { arm_body(P, tstop, budget); }
+__global__ void k_begin(Params P) {
+  pdl_enter();
+  begin_body(P);
+}
+__global__ void k_end(Params P) {
+  pdl_enter();
+  end_body(P);
+}
+__global__ void k_arm(Params P, double tstop, double budget) {
+  pdl_enter();
+  arm_body(P, tstop, budget);
+}
 
 // S_PSNZ <- 1 if p_S of either state buffer is nonzero at a point the AB2
 // stage reads (every point but the last plane of each axis)
 __global__ void k_ps_check(Params P) {
+  pdl_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
   bool nz = false;
   if (i < P.N[0] - 1 && j < P.N[1] - 1 && k < P.N[2] - 1) {
@@ -1115,6 +1135,7 @@ __global__ void k_ps_check(Params P) {
 
 template <int COORD, bool BG>
 __global__ void k_dt(Params P) {
+  pdl_enter();
   double dtc = DBL_MAX, db = 0.0;
   dt_body<COORD, BG>(P, grid_pos(), dtc, db);
   block_commit(dtc, db, P.scal + S_NEXT_DT, P.scal + S_DIVB);
@@ -1125,6 +1146,7 @@ __global__ void k_dt(Params P) {
 // src/solver_func.c:308-343, src/spherical/spherical_general.c:700-743);
 // thread (i, band row, k)
 __global__ void k_ring_dt(Params P) {
+  pdl_enter();
   double dtc = DBL_MAX, db = 0.0;
   const int i = NGH + blockIdx.x * blockDim.x + threadIdx.x;
   const int k = NGH + blockIdx.z * blockDim.z + threadIdx.z;
@@ -1167,42 +1189,50 @@ __global__ void k_ring_dt(Params P) {
 
 template <typename R, bool PSL>
 __global__ void __launch_bounds__(256, GOP_MINB(AB2, R)) k_ab2(Params P, Work<R> w) {
+  pdl_enter();
   if (stopped(P)) return;
   ab2_body<R, PSL>(P, w, grid_pos());
 }
 template <typename R, int D>
 __global__ void __launch_bounds__(256, GOP_MINB(C2C, R)) k_c2c(Params P, Work<R> w) {
+  pdl_enter();
   if (stopped(P)) return;
   c2c_body<R, D>(P, w, grid_pos());
 }
 // BG: with the background-field terms (Params::bg set)
 template <typename R, int D, bool BG>
 __global__ void __launch_bounds__(256, GOP_MINB(EMF, R)) k_emf(Params P, Work<R> w) {
+  pdl_enter();
   if (stopped(P)) return;
   emf_body<R, D, BG>(P, w, grid_pos());
 }
 template <typename R, int D, bool BG, bool PSL>
 __global__ void __launch_bounds__(256, GOP_MINB(FLUX, R)) k_flux(Params P, Work<R> w) {
+  pdl_enter();
   if (stopped(P)) return;
   flux_body<R, D, BG, PSL>(P, w, grid_pos());
 }
 template <int COORD, typename R>
 __global__ void __launch_bounds__(256, GOP_MINB_CT) k_ct(Params P, Work<R> w) {
+  pdl_enter();
   if (stopped(P)) return;
   ct_body<COORD, R>(P, w, grid_pos());
 }
 template <int COORD, typename R, bool BG, bool PSL>
 __global__ void __launch_bounds__(256, GOP_UPD_MINB(COORD, R)) k_update(Params P, Work<R> w) {
+  pdl_enter();
   if (stopped(P)) return;
   double dtc = DBL_MAX, db = 0.0;
   update_body<COORD, R, BG, PSL>(P, w, grid_pos(), dtc, db);
   block_commit(dtc, db, P.scal + S_NEXT_DT, P.scal + S_DIVB);
 }
 __global__ void k_wrap(Params P, int axis, int which) {
+  pdl_enter();
   if (stopped(P)) return;
   wrap_body(P, axis, which, grid_pos());
 }
 __global__ void k_bcface(Params P, int axis, int side, int kind, int gkind, int which) {
+  pdl_enter();
   if (stopped(P)) return;
   bcface_body(P, axis, side, kind, gkind, which, grid_pos());
 }
@@ -1211,6 +1241,7 @@ __global__ void k_bcface(Params P, int axis, int side, int kind, int gkind, int 
 
 // reference layout [f][i][j][k] (k fastest) <-> device layout
 __global__ void k_from_ref(Params P, int nf, const double* __restrict__ src, double* __restrict__ dst) {
+  pdl_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int kf = blockIdx.z;
@@ -1221,6 +1252,7 @@ __global__ void k_from_ref(Params P, int nf, const double* __restrict__ src, dou
 }
 
 __global__ void k_to_ref(Params P, int nf, const double* __restrict__ src, double* __restrict__ dst) {
+  pdl_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int kf = blockIdx.z;
@@ -1232,6 +1264,7 @@ __global__ void k_to_ref(Params P, int nf, const double* __restrict__ src, doubl
 
 template <typename R>
 __global__ void k_widen(Params P, int nf, const R* __restrict__ src, double* __restrict__ dst) {
+  pdl_enter();
   const size_t n = (size_t)nf * P.fs;
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
     dst[t] = (double)src[t];
@@ -1239,6 +1272,7 @@ __global__ void k_widen(Params P, int nf, const R* __restrict__ src, double* __r
 
 // mags over the ghost range from face fields (for downloads)
 __global__ void k_mags(Params P, const double* __restrict__ B, double* __restrict__ out) {
+  pdl_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z * blockDim.z + threadIdx.z;
@@ -1258,10 +1292,19 @@ static dim3 grid3(int a, int b, int c, dim3 blk) {
   return dim3((a + blk.x - 1) / blk.x, (b + blk.y - 1) / blk.y, (c + blk.z - 1) / blk.z);
 }
 
-#define LAUNCH(kern, grd, blk, st, ...)            \
-  do {                                             \
-    kern<<<grd, blk, 0, st>>>(__VA_ARGS__);        \
-    g_launches++;                                  \
+#define LAUNCH(kern, grd, blk, st, ...)                                          \
+  do {                                                                           \
+    cudaLaunchAttribute at_[1];                                                  \
+    at_[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;              \
+    at_[0].val.programmaticStreamSerializationAllowed = 1;                       \
+    cudaLaunchConfig_t cfg_ = {};                                                \
+    cfg_.gridDim = dim3(grd);                                                    \
+    cfg_.blockDim = dim3(blk);                                                   \
+    cfg_.stream = st;                                                            \
+    cfg_.attrs = at_;                                                            \
+    cfg_.numAttrs = 1;                                                           \
+    cudaLaunchKernelEx(&cfg_, kern, __VA_ARGS__);                                \
+    g_launches++;                                                                \
   } while (0)
 
 Tune::Tune() {
