@@ -175,6 +175,34 @@ def test_spherical_shell_matches_oracle(gop, oracle_mod):
     compare(n, d["gas"], d["face_b"], ref["W"], ref["B"], TOL_FP64, "spherical shell")
 
 
+@pytest.mark.parametrize("case", [
+    dict(coord=0, n=(77, 45, 21), bc="sfrepp", steps=6),
+    dict(coord=2, n=(67, 35, 19), bc="eeeeee", steps=5),
+], ids=["blast_77x45x21", "sphere_67x35x19"])
+def test_ragged_sizes_match_oracle(gop, oracle_mod, case):
+    """Grid sizes that fill no launch block evenly in any direction (the
+    last blocks along every axis are partial; the spherical case also runs
+    the separate constrained-transport launch), against the C restatement."""
+    n, coord = case["n"], case["coord"]
+    if coord == 0:
+        x = [gop.grid_uniform(m, -0.5, 0.5) for m in n]
+        inst = gop.Instance(n, *x, bc=case["bc"])
+        W0, B0 = inst.init_problem(gop.PROBLEM_BLAST, b=(0.4, 0.5, 0.3), center=(0.05, -0.1, 0.02))
+    else:
+        dom = (1.0, 2.0, 0.25 * math.pi, 0.75 * math.pi, -0.25 * math.pi, 0.25 * math.pi)
+        x = [gop.grid_uniform(n[a], dom[2 * a], dom[2 * a + 1]) for a in range(3)]
+        inst = gop.Instance(n, *x, coord=gop.COORD_SPHERICAL, bc=case["bc"])
+        W0, B0 = inst.init_problem(gop.PROBLEM_LOOP_SPH, loop=(1.4, 0.1, 0.3, 1e-3))
+    inst.upload(W0, B0)
+    inst.prepare()
+    inst.step(case["steps"])
+    d = inst.download(("gas", "face_b"))
+    ref = run_oracle(oracle_mod, n, x, coord, case["bc"], W0, B0, case["steps"])
+    compare(n, d["gas"], d["face_b"], ref["W"], ref["B"], TOL_FP64, str(n))
+    assert math.isclose(inst.stats()["time"], ref["time"], rel_tol=1e-12)
+    inst.close()
+
+
 def test_div_b_stays_at_roundoff_and_mass_is_conserved(gop):
     n = (48, 48, 48)
     inst = gop.make(gop.PROBLEM_BLAST, n, b=(0.5, 0.4, 0.3))
