@@ -850,7 +850,10 @@ static int enqueue_steps(gop_instance* h, int nsteps, double time_stop) {
     hook.ctx = h;
   }
   launch_arm(P, time_stop, (double)nsteps, h->st);
-  if (!h->prof && nsteps > 1) {  // replay the captured step
+  // inside a caller's stream capture the launches go straight into it
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(h->st, &cap));
+  if (!h->prof && nsteps >= 1 && cap == cudaStreamCaptureStatusNone) {  // replay the captured step
     int rc = capture_step(h);
     if (rc) return rc;
     // with a stop time and many steps, look at the stop flag between

@@ -129,7 +129,10 @@ int gop_prepare(gop_instance *h, int restart);
  * respect to the host unless time_out is non-NULL, or unless time_stop is
  * finite and nsteps > 256: the call then looks at the stop flag every 256
  * steps (synchronising the stream) so it returns soon after time_stop.
- * More than one step replays a captured CUDA graph of a step. */
+ * Steps replay a CUDA graph of one step, captured at the first call (and
+ * again after gop_prepare changes the kernels, gop_set_background or
+ * gop_autotune); with gop_set_profiling on, or while the instance's stream
+ * is being captured by the caller, they are launched one by one. */
 int gop_step(gop_instance *h, int nsteps, double time_stop, double *time_out);
 
 /* Copies the state back in the reference layout: any pointer may be NULL.
