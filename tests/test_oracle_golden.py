@@ -66,3 +66,46 @@ def test_oracle_detects_planted_error(oracle_mod):
     n, st = run_oracle(oracle_mod, g)
     sl = tuple(slice(NG, NG + m) for m in n)
     assert not np.array_equal(st["W"][(0,) + sl], g["W1"][0][:-1, :-1, :-1])
+
+
+@pytest.mark.parametrize("case", [
+    dict(n=(12, 10, 8), coord="cart", problem="blast", bc="ssrrfe", steps=8,
+         domain=(-0.5, 0.5, -0.5, 0.5, -0.5, 0.5),
+         env={"GOP_PS": "0.2", "GOP_CENTER": "0.1,-0.05,0.0", "GOP_B": "0.3,0.5,0.2"}),
+    dict(n=(12, 10, 8), coord="sph", problem="loop_sph", bc="eeeeee", steps=6,
+         domain=(1.0, 2.0, 0.7853981633974483, 2.356194490192345, -0.7853981633974483,
+                 0.7853981633974483),
+         env={"GOP_PS": "0.5", "GOP_LOOP": "1.5,0,0.3,1e-3"}),
+], ids=["blast_bcmix_entropy", "loop_sph_entropy"])
+def test_oracle_entropy_channel_matches_reference(oracle_mod, case):
+    """A live entropy channel (p_S = f * p, GOP_PS in the oracle's problem
+    file) through the restatement and through GAMERA-OP's own solver, from
+    the reference's step-0 state: bit for bit, p_S included.  This pins the
+    checker of the GPU tests that feed p_S through boundary ghosts."""
+    ref_run = pytest.importorskip("ref_run")
+    if not ref_run.available(case["coord"], "strict"):
+        pytest.skip("reference binary not built")
+    env = {"GOP_BC": case["bc"], "GOP_DOMAIN": ",".join(repr(v) for v in case["domain"]),
+           **case["env"]}
+    ref = ref_run.run(case["n"], case["steps"], problem=case["problem"], coord=case["coord"],
+                      env=env, timeout=300)
+    s0, s1 = ref.state(0), ref.state(-1)
+    W0 = np.stack([s0[k] for k in ("rho", "v1", "v2", "v3", "p", "pS")])
+    B0 = np.stack([s0[k] for k in ("bi", "bj", "bk")])
+    n = case["n"]
+    d0 = ref.dumps[0]  # the reference's own face coordinates
+    xs = [np.asarray(d0["x1"])[:, 0, 0], np.asarray(d0["x2"])[0, :, 0], np.asarray(d0["x3"])[0, 0, :]]
+    o = oracle_mod.Oracle(n, *xs, coord=0 if case["coord"] == "cart" else 2, bc=case["bc"])
+    o.set_state(W0, B0)
+    o.prepare()
+    o.run(case["steps"])
+    st = o.state()
+    act = tuple(slice(NG, NG + m) for m in n)
+    assert np.abs(W0[5][act]).min() > 0.0
+    for m, k in enumerate(("rho", "v1", "v2", "v3", "p", "pS")):
+        assert np.array_equal(st["W"][m][act], s1[k][act]), k
+    for a, k in enumerate(("bi", "bj", "bk")):
+        s = list(act)
+        s[a] = slice(NG, NG + n[a] + 1)
+        assert np.array_equal(st["B"][a][tuple(s)], s1[k][tuple(s)]), k
+    assert st["time"] == s1["time"]
