@@ -766,7 +766,7 @@ int gop_prepare(gop_instance* h, int restart) {
   s[S_PSNZ] = 0.0;
   CK(cudaMemcpyAsync(h->scal, s, NSCAL * sizeof(double), cudaMemcpyHostToDevice, h->st));
   // CFL dt and div B of the initial state (src/solver_solve.c:94-98)
-  launch_dt(P, h->d.coord, h->st);
+  launch_dt(P, h->d.coord, h->d.precision == GOP_PREC_MIXED, h->st);
   // is the entropy channel live?  A p_S that is zero in the state and its
   // history stays zero in every later step, and the flux kernels skip it
   launch_ps_check(P, h->st);

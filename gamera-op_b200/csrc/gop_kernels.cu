@@ -935,8 +935,12 @@ __device__ __forceinline__ void update_body(const Params& P, const Work<R>& wk, 
   }
 }
 
-// CFL dt and |div B| of one cell of the current state (prepare)
-template <int COORD, bool BG>
+// CFL dt and |div B| of one cell of the current state (prepare).  The dt
+// takes the form and arithmetic R of the step's own estimate (the
+// Cartesian update's 1/dx from the face area over the volume; the FP32
+// estimate on the mixed path; FP64 in the rows of the pole ring average),
+// so a restarted run takes exactly the step the uninterrupted one would.
+template <int COORD, bool BG, typename R>
 __device__ __forceinline__ void dt_body(const Params& P, Pos t, double& dtc, double& db) {
   const int i = NGH + t.x, j = NGH + t.y, k = NGH + t.z;
   if (i >= NGH + P.n[0] || j >= NGH + P.n[1] || k >= NGH + P.n[2]) return;
@@ -950,8 +954,27 @@ __device__ __forceinline__ void dt_body(const Params& P, Pos t, double& dtc, dou
     b2 += P.bg[(size_t)(BG_B0 + 1) * P.fs + c];
     b3 += P.bg[(size_t)(BG_B0 + 2) * P.fs + c];
   }
-  dtc = cfl_cell<COORD>(P, i, j, k, W[c], W[c + P.fs], W[c + 2 * P.fs], W[c + 3 * P.fs],
-                        W[c + 4 * P.fs], b1, b2, b3);
+  if constexpr (COORD == 0) {  // as update_cart
+    const double dx[3] = {tb(P, 0, T_DX, i), tb(P, 1, T_DX, j), tb(P, 2, T_DX, k)};
+    const double A[3] = {dx[1] * dx[2], dx[0] * dx[2], dx[0] * dx[1]};
+    const double ivol = 1.0 / (dx[0] * dx[1] * dx[2]);
+    const double il[3] = {A[0] * ivol, A[1] * ivol, A[2] * ivol};
+    const R r = (R)W[c], u = (R)W[c + P.fs], v = (R)W[c + 2 * P.fs], w = (R)W[c + 3 * P.fs];
+    const R p = (R)W[c + 4 * P.fs];
+    const R bsq = (R)(b1 * b1 + b2 * b2 + b3 * b3);
+    const R va = sqrt(bsq / r);
+    const R vae = va * (R)P.ca / sqrt(va * va + (R)P.ca2);
+    const R vf = sqrt(u * u + v * v + w * w);
+    const R vs = sqrt((R)P.gamma * p / r);
+    const R vc = vf + sqrt(vs * vs + vae * vae);
+    dtc = (double)((R)P.cfl / (vc * (R)il[0] + vc * (R)il[1] + vc * (R)il[2]));
+  } else if (P.ring && ring_band_row(P, j)) {  // as k_ring_dt
+    dtc = cfl_cell<COORD>(P, i, j, k, W[c], W[c + P.fs], W[c + 2 * P.fs], W[c + 3 * P.fs],
+                          W[c + 4 * P.fs], b1, b2, b3);
+  } else {  // as the curvilinear update
+    dtc = cfl_cell<COORD, R>(P, i, j, k, W[c], W[c + P.fs], W[c + 2 * P.fs], W[c + 3 * P.fs],
+                             W[c + 4 * P.fs], b1, b2, b3);
+  }
   const double vol = Geo<COORD>::vol(P, i, j, k);
   double d = 0.0;
 #pragma unroll
@@ -1133,11 +1156,11 @@ __global__ void k_ps_check(Params P) {
   if (__any_sync(0xffffffffu, nz) && (threadIdx.x & 31) == 0) P.scal[S_PSNZ] = 1.0;
 }
 
-template <int COORD, bool BG>
+template <int COORD, bool BG, typename R>
 __global__ void k_dt(Params P) {
   pdl_enter();
   double dtc = DBL_MAX, db = 0.0;
-  dt_body<COORD, BG>(P, grid_pos(), dtc, db);
+  dt_body<COORD, BG, R>(P, grid_pos(), dtc, db);
   block_commit(dtc, db, P.scal + S_NEXT_DT, P.scal + S_DIVB);
 }
 
@@ -1359,17 +1382,23 @@ void launch_ps_check(const Params& P, cudaStream_t st) {
   LAUNCH(k_ps_check, dim3((nx + blk.x - 1) / blk.x, P.N[1] - 1, P.N[2] - 1), blk, st, P);
 }
 
-void launch_dt(const Params& P, int coord, cudaStream_t st) {
+template <typename R>
+static void launch_dt_r(const Params& P, int coord, cudaStream_t st) {
   const dim3 blk(32, 4, 2);
   const dim3 g = grid3(P.n[0], P.n[1], P.n[2], blk);
   const bool bg = P.bg != nullptr;
   if (coord == 0) {
-    if (bg) LAUNCH((k_dt<0, true>), g, blk, st, P);
-    else LAUNCH((k_dt<0, false>), g, blk, st, P);
+    if (bg) LAUNCH((k_dt<0, true, R>), g, blk, st, P);
+    else LAUNCH((k_dt<0, false, R>), g, blk, st, P);
   } else {
-    if (bg) LAUNCH((k_dt<2, true>), g, blk, st, P);
-    else LAUNCH((k_dt<2, false>), g, blk, st, P);
+    if (bg) LAUNCH((k_dt<2, true, R>), g, blk, st, P);
+    else LAUNCH((k_dt<2, false, R>), g, blk, st, P);
   }
+}
+
+void launch_dt(const Params& P, int coord, bool mixed, cudaStream_t st) {
+  if (mixed) launch_dt_r<float>(P, coord, st);
+  else launch_dt_r<double>(P, coord, st);
 }
 
 template <typename R, bool BG>

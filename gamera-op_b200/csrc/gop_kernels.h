@@ -68,7 +68,9 @@ void launch_begin(const Params& P, cudaStream_t st);
 void launch_end(const Params& P, cudaStream_t st);
 // arm a gop_step call: stop after time tstop or after `budget` steps
 void launch_arm(const Params& P, double tstop, double budget, cudaStream_t st);
-void launch_dt(const Params& P, int coord, cudaStream_t st);
+// CFL dt (in the form and arithmetic of the step's own estimate) and
+// max|div B| of the current state
+void launch_dt(const Params& P, int coord, bool mixed, cudaStream_t st);
 // P.scal[S_PSNZ] <- 1 if p_S is nonzero in either state buffer (it must be 0 before)
 void launch_ps_check(const Params& P, cudaStream_t st);
 template <typename R>

@@ -219,17 +219,23 @@ def test_div_b_stays_at_roundoff_and_mass_is_conserved(gop):
     assert abs(m1 - m0) / m0 < 1e-13
 
 
-def test_restart_continues_bit_identically(gop):
+@pytest.mark.parametrize("prec,first", [(0, 10), (1, 11)], ids=["fp64", "mixed_odd_parity"])
+def test_restart_continues_bit_identically(gop, prec, first):
+    """Download the state and its AB2 history mid-run, upload both into a
+    fresh instance and prepare it for a restart: the next steps are
+    bit-identical to the uninterrupted run.  gop_prepare takes the first dt
+    in the form and arithmetic of the step's own estimate (FP32 on the mixed
+    path), so the restarted run takes the same step."""
     n = (24, 24, 24)
-    a = gop.make(gop.PROBLEM_BLAST, n, b=(0.5, 0.4, 0.3))
+    a = gop.make(gop.PROBLEM_BLAST, n, b=(0.5, 0.4, 0.3), precision=prec)
     a.prepare()
-    a.step(10)
+    a.step(first)
     mid = a.download(("gas", "face_b", "gas_p", "face_b_p"))
     sa = a.stats()
     a.step(10)
     full = a.download(("gas", "face_b"))
     x = [gop.grid_uniform(m, -0.5, 0.5) for m in n]
-    b = gop.Instance(n, *x)
+    b = gop.Instance(n, *x, precision=prec)
     b.upload(mid["gas"], mid["face_b"], mid["gas_p"], mid["face_b_p"], time=sa["time"], dt0=sa["dt0"])
     b.prepare(restart=True)
     b.step(10)
