@@ -177,8 +177,12 @@ def run_reference(args, rank):
     line.update({
         "value": round(v, 4), "ms_per_step": round(t / args.steps * 1e3, 3),
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "blast3d_periodic_fp64", "grid": list(n),
-                   "note": "bounded sample of the 256^3 workload (same problem at 64^3)"},
+        "config": {"workload": f"blast3d_periodic_{args.n}^3_{args.precision}",
+                   "grid": [args.n] * 3,
+                   "problem": "blast p_in=10 p_out=0.1 r=0.1 B=(1/sqrt2,1/sqrt2,0) gamma=5/3 CFL=0.3",
+                   "sample_grid": list(n),
+                   "note": f"bounded sample: each step of the {args.n}^3 workload timed on the "
+                           f"same problem at 64^3 (the reference computes in FP64)"},
         "latency_ms": {"p50": round(float(np.percentile(durs, 50)), 3),
                        "p99": round(float(np.percentile(durs, 99)), 3)},
         "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": thr, "kind": "reference",

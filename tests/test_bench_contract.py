@@ -48,3 +48,6 @@ def test_reference_arm_prints_one_contract_line():
     assert d["cpu_baseline"]["value"] == d["value"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
+    # the same workload as the CUDA arm's default line, timed on a bounded sample
+    assert d["config"]["workload"] == "blast3d_periodic_256^3_fp64"
+    assert d["config"]["sample_grid"] == [64, 64, 64]
