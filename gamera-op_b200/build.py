@@ -15,6 +15,7 @@ LIB = PKG / "libgamera_op.so"
 SOURCES = [
     PKG / "csrc" / "gop_api.cu",
     PKG / "csrc" / "gop_kernels.cu",
+    PKG / "csrc" / "gop_sweep.cu",
     PKG / "csrc" / "gop_noalloc.cu",
     PKG / "csrc" / "gop_init.cu",
     PKG / "csrc" / "gop_ring.cu",
@@ -23,6 +24,7 @@ SOURCES = [
 ]
 HEADERS = [ROOT / "include" / "gamera_op.h", PKG / "csrc" / "gop_device.cuh",
            PKG / "csrc" / "gop_kernels.h", PKG / "csrc" / "gop_internal.h",
+           PKG / "csrc" / "gop_stage.cuh", PKG / "csrc" / "gop_tma.cuh",
            PKG / "csrc" / "gop_fields.h"]
 
 NVCC_FLAGS = [

@@ -386,6 +386,7 @@ struct gop_instance {
   Work<double> wd;
   Work<float> wf;
   Tune tune;
+  SweepSet* sweep = nullptr;  // tensor maps of the tile-staged flux sweeps
   cudaGraphExec_t step_graph = nullptr;  // one captured step (replayed by gop_step)
   uint64_t gen = 0;                      // bumped whenever a step's launches change
   int64_t step_nodes = 0;
@@ -603,6 +604,9 @@ int gop_create(const gop_desc* desc, gop_instance** out) {
     for (int t = 0; t < 16; t++) P.nchunk[t] = r.nchunk[t];
     P.ringtab = h->ringtab;
   }
+  // the tile-staged flux sweeps read the work and state arrays through
+  // tensor maps made once here; without them the per-face kernels run
+  h->sweep = mixed ? sweep_create<float>(P, h->wf) : sweep_create<double>(P, h->wd);
   cudaError_t le = e != cudaSuccess ? e : cudaStreamSynchronize(h->st);
   if (le == cudaSuccess) le = cudaGetLastError();
   if (le != cudaSuccess) {
@@ -621,6 +625,7 @@ int gop_destroy(gop_instance* h) {
                   (void*)h->staging, (void*)h->bg, (void*)h->ringtab})
     if (p) cudaFreeAsync(p, h->st);
   if (h->own) cudaStreamDestroy(h->own);  // released once the frees have run
+  sweep_destroy(h->sweep);
   delete[] h->hscal;
   prof_collect(h);
   for (cudaEvent_t e : h->pool) cudaEventDestroy(e);
@@ -805,9 +810,9 @@ static void enqueue_one_step(gop_instance* h, cudaStream_t st, const Hook& hook)
   launch_begin(P, st);
   hook(G_BEGIN, 0);
   if (h->d.precision == GOP_PREC_MIXED)
-    launch_step_body<float>(P, h->d.coord, h->wf, st, h->tune, hook);
+    launch_step_body<float>(P, h->d.coord, h->wf, st, h->tune, h->sweep, hook);
   else
-    launch_step_body<double>(P, h->d.coord, h->wd, st, h->tune, hook);
+    launch_step_body<double>(P, h->d.coord, h->wd, st, h->tune, h->sweep, hook);
   hook(G_GHOST, 1);
   launch_ghosts(P, h->d.bc, h->d.gem_bc, 0, st);
   hook(G_GHOST, 0);
@@ -888,6 +893,8 @@ int gop_step(gop_instance* h, int nsteps, double time_stop, double* time_out) {
     CK(cudaMemcpyAsync(h->hscal, h->scal, NSCAL * sizeof(double), cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
     *time_out = h->hscal[S_TIME];
+    if (h->hscal[S_FLAGS] == 2.0)
+      return fail(GOP_ECUDA, "a tile pipeline wait on the device timed out");
     if (h->hscal[S_FLAGS] != 0.0) return fail(GOP_ENUMERIC, "non-finite or non-positive state");
   }
   return GOP_OK;
@@ -984,13 +991,18 @@ int gop_autotune(gop_instance* h, int reps, int* chosen) {
   for (int slot = 0; slot < NTUNE; slot++) {
     float best = 1e30f;
     int best_c = 0;
-    for (int c = 0; c < ncand; c++) {
-      if (cand[c].x * cand[c].y * cand[c].z > 256) continue;
+    // the flux slots also try the tile-staged sweep kernel (candidate ncand)
+    const bool flux = slot >= K_FLUX0 && slot <= K_FLUX2;
+    const bool try_sweep = flux && h->sweep && !P.ps_live;
+    for (int c = 0; c < ncand + (try_sweep ? 1 : 0); c++) {
+      const bool sw = c == ncand;
+      if (!sw && cand[c].x * cand[c].y * cand[c].z > 256) continue;
+      const dim3 blk = sw ? h->tune.blk[slot] : cand[c];
       // warm-up launch, then reps timed launches
       for (int r = 0; r <= reps; r++) {
         if (r == 1) cudaEventRecord(a, h->st);
-        if (mixed) launch_slot<float>(h->P, h->d.coord, h->wf, slot, cand[c], h->st);
-        else launch_slot<double>(h->P, h->d.coord, h->wd, slot, cand[c], h->st);
+        if (mixed) launch_slot<float>(h->P, h->d.coord, h->wf, slot, blk, h->st, sw ? h->sweep : nullptr);
+        else launch_slot<double>(h->P, h->d.coord, h->wd, slot, blk, h->st, sw ? h->sweep : nullptr);
       }
       cudaEventRecord(b, h->st);
       CK(cudaEventSynchronize(b));
@@ -1001,7 +1013,8 @@ int gop_autotune(gop_instance* h, int reps, int* chosen) {
         best_c = c;
       }
     }
-    h->tune.blk[slot] = cand[best_c];
+    if (best_c < ncand) h->tune.blk[slot] = cand[best_c];
+    if (flux) h->tune.flux_sweep[slot - K_FLUX0] = best_c == ncand;
     if (chosen) chosen[slot] = best_c;
     drop_step_graph(h);  // the captured step has the old shapes
   }
@@ -1015,6 +1028,15 @@ int gop_autotune(gop_instance* h, int reps, int* chosen) {
   cudaFreeAsync(hist, h->st);
   CK(cudaStreamSynchronize(h->st));
   CK(cudaGetLastError());
+  return GOP_OK;
+}
+
+int gop_set_sweep(gop_instance* h, int on) {
+  if (!h) return fail(GOP_EINVAL, "instance is NULL");
+  if (on && !h->sweep) return fail(GOP_ENODEV, "the tile-staged sweep kernels are not available");
+  CK(cudaStreamSynchronize(h->st));
+  for (int d = 0; d < 3; d++) h->tune.flux_sweep[d] = on != 0;
+  drop_step_graph(h);
   return GOP_OK;
 }
 
@@ -1051,7 +1073,7 @@ int gop_get_stats(gop_instance* h, gop_stats* out) {
   out->dt0 = s[S_DT0];
   out->divb_max = s[S_DIVB];
   out->steps = (int64_t)s[S_STEPS];
-  out->flags = s[S_FLAGS] != 0.0 ? 1 : 0;
+  out->flags = s[S_FLAGS] == 2.0 ? 2 : (s[S_FLAGS] != 0.0 ? 1 : 0);
   out->reserved = 0;
   out->device_bytes = h->bytes;
   return GOP_OK;
@@ -1270,6 +1292,7 @@ int gop_batch_wait(gop_batch* b) {
     double* sc = h->hscal;
     CK(cudaMemcpyAsync(sc, h->scal, NSCAL * sizeof(double), cudaMemcpyDeviceToHost, b->st));
     CK(cudaStreamSynchronize(b->st));
+    if (sc[S_FLAGS] == 2.0) return fail(GOP_ECUDA, "a tile pipeline wait on the device timed out");
     if (sc[S_FLAGS] != 0.0) return fail(GOP_ENUMERIC, "non-finite or non-positive state in a member");
   }
   return GOP_OK;

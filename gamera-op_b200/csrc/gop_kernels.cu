@@ -25,6 +25,7 @@
 // in both.
 #include "gop_device.cuh"
 #include "gop_kernels.h"
+#include "gop_stage.cuh"
 
 #include <algorithm>
 #include <atomic>
@@ -32,21 +33,9 @@
 
 namespace gop {
 
-enum { RHO = 0, V1, V2, V3, PR, PS };
 
 // ------------------------------------------------------------------ utils
 
-__device__ __forceinline__ bool stopped(const Params& P) { return P.scal[S_STOP] != 0.0; }
-
-// Programmatic dependent launch: LAUNCH lets each kernel start launching
-// while its predecessor on the stream is still running.  Every kernel it
-// launches first waits here until that predecessor has completed and its
-// writes are visible, then lets its own successor start launching, so only
-// launch latency and block scheduling overlap, never the work.
-__device__ __forceinline__ void pdl_enter() {
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
 
 __device__ __forceinline__ void atomic_min_pos(double* slot, double v) {
   // positive doubles order like their bit patterns
@@ -142,22 +131,7 @@ __device__ __forceinline__ void line8(const T* __restrict__ a, long long s, R v[
   for (int t = 0; t < 8; t++) v[t] = (R)a[(t - 4) * s];
 }
 
-__device__ __forceinline__ double rsq(double x) { return rsqrt(x); }
-__device__ __forceinline__ float rsq(float x) { return rsqrtf(x); }
 
-// The step-start state the PDM limiters compare against, in the stage type:
-// the FP64 state itself on the plain path, its FP32 copy (written by the
-// AB2 stage) on the mixed path.
-template <typename R>
-__device__ __forceinline__ const R* lim_w(const Params& P, const Work<R>& wk) {
-  if constexpr (sizeof(R) == 8) return reinterpret_cast<const R*>(P.Wbuf[cur_buf(P)]);
-  else return wk.Wl;
-}
-template <typename R>
-__device__ __forceinline__ const R* lim_b(const Params& P, const Work<R>& wk) {
-  if constexpr (sizeof(R) == 8) return reinterpret_cast<const R*>(P.Bbuf[cur_buf(P)]);
-  else return wk.Bl;
-}
 
 // thread coordinates in a launch space
 struct Pos {
@@ -353,112 +327,6 @@ __device__ __forceinline__ void emf_body(const Params& P, const Work<R>& wk, Pos
 
 // ------------------------------------------------------------ face flux
 
-// Rusanov hydro flux and Maxwell stress at the face normal to D at cell x
-// from the reconstructed states (src/solver_func.c:934-1529).  F[9] =
-// mass, 3 momenta, energy, entropy, 3 stress components.  Also writes the
-// first centre-to-edge sweep of edges along (D+2)%3 (see c2c_body).
-template <typename R, int D, bool BG, bool PSL>
-__device__ __forceinline__ void flux_out(const Params& P, const Work<R>& wk, long long x,
-                                         const R L[6], const R Rt[6], const R mL[3],
-                                         const R mR[3]) {
-  const size_t fs = P.fs;
-  // background field averaged over this face (B0Aface*_b1..3; the normal
-  // component is B0Aface*_bn)
-  R b0[3] = {R(0), R(0), R(0)};
-  if constexpr (BG) {
-#pragma unroll
-    for (int a = 0; a < 3; a++) b0[a] = (R)P.bg[(size_t)(BG_FACE + 3 * D + a) * fs + x];
-  }
-  const R gm = (R)P.gamma, gm1 = (R)P.gm1, ca = (R)P.ca, ca2 = (R)P.ca2;
-  const R rl = L[RHO], rr = Rt[RHO], pl = L[PR], pr = Rt[PR], sl = L[PS], sr = Rt[PS];
-  const R irl = R(1) / rl, irr = R(1) / rr;
-  const R csl = sqrt(gm * pl * irl), csr = sqrt(gm * pr * irr);
-  // entropy channel: p_S = 0 everywhere unless a problem sets it; the
-  // zero test only skips exact zeros
-
-  const R btl = mL[0] * mL[0] + mL[1] * mL[1] + mL[2] * mL[2];
-  const R btr = mR[0] * mR[0] + mR[1] * mR[1] + mR[2] * mR[2];
-  // |B + B0|^2 of either state: the Alfven speed and the Boris term see the
-  // total field
-  R ttl = btl, ttr = btr;
-  if constexpr (BG) {
-    ttl = (mL[0] + b0[0]) * (mL[0] + b0[0]) + (mL[1] + b0[1]) * (mL[1] + b0[1]) +
-          (mL[2] + b0[2]) * (mL[2] + b0[2]);
-    ttr = (mR[0] + b0[0]) * (mR[0] + b0[0]) + (mR[1] + b0[1]) * (mR[1] + b0[1]) +
-          (mR[2] + b0[2]) * (mR[2] + b0[2]);
-  }
-  const R val = sqrt(ttl * irl), var = sqrt(ttr * irr);
-  const R vel = val * ca * rsq(val * val + ca2);
-  const R ver = var * ca * rsq(var * var + ca2);
-  const R vnl = L[V1 + D], vnr = Rt[V1 + D];
-  const R vf = fmax(fabs(vnl) + sqrt(csl * csl + vel * vel), fabs(vnr) + sqrt(csr * csr + ver * ver));
-  R mol[3], mor[3];
-#pragma unroll
-  for (int a = 0; a < 3; a++) {
-    mol[a] = rl * L[V1 + a];
-    mor[a] = rr * Rt[V1 + a];
-  }
-  const R igm1 = (R)P.inv_gm1;
-  const R el = R(0.5) * rl * (L[V1] * L[V1] + L[V2] * L[V2] + L[V3] * L[V3]) + pl * igm1;
-  const R er = R(0.5) * rr * (Rt[V1] * Rt[V1] + Rt[V2] * Rt[V2] + Rt[V3] * Rt[V3]) + pr * igm1;
-
-  // the first centre-to-edge sweep for edges along E = (D+2)%3: velocity
-  // components D and (D+1)%3 along D, averaged (see c2c_body)
-  {
-    constexpr int E = (D + 2) % 3, c1 = (D + 1) % 3;
-    wk.V[x + (size_t)(2 * E) * fs] = R(0.5) * (L[V1 + D] + Rt[V1 + D]);
-    wk.V[x + (size_t)(2 * E + 1) * fs] = R(0.5) * (L[V1 + c1] + Rt[V1 + c1]);
-  }
-  R* o = wk.F + (size_t)(9 * D) * fs + x;
-  o[0] = R(0.5) * (mol[D] + mor[D] - vf * (rr - rl));
-#pragma unroll
-  for (int a = 0; a < 3; a++) {
-    R u = mol[a] * vnl + mor[a] * vnr - vf * (mor[a] - mol[a]);
-    if (a == D) u = mol[a] * vnl + pl + mor[a] * vnr + pr - vf * (mor[a] - mol[a]);
-    o[(1 + a) * fs] = R(0.5) * u;
-  }
-  o[4 * fs] = R(0.5) * (el * vnl + pl * vnl + er * vnr + pr * vnr - vf * (er - el));
-  // entropy channel (p_S = 0 unless a problem sets it): with zero left and
-  // right states its flux is zero and the update leaves p_S at +0 either way
-  R fS = R(0);
-  if (sl != R(0) || sr != R(0)) {
-    const R csel = sl == R(0) ? R(0) : sqrt(gm * sl * irl);
-    const R cser = sr == R(0) ? R(0) : sqrt(gm * sr * irr);
-    const R vfe = fmax(fabs(vnl) + sqrt(csel * csel + vel * vel), fabs(vnr) + sqrt(cser * cser + ver * ver));
-    const R Sl = (sl == R(0) && rl > R(0)) ? sl : sl / pow(rl, gm1);
-    const R Sr = (sr == R(0) && rr > R(0)) ? sr : sr / pow(rr, gm1);
-    fS = R(0.5) * (Sl * vnl + Sr * vnr - vfe * (Sr - Sl));
-  }
-  if constexpr (PSL) o[5 * fs] = fS;  // else the update takes a zero divergence
-  const R bn = lim_b<R>(P, wk)[x + D * fs];
-  const R bq = (ttl + ttr) * (R)P.q_ca;
-  if constexpr (BG) {
-    // stress of B^2 + 2 B.B0 with the B0 cross terms
-    // (src/solver_func.c:1268-1333)
-    const R bsl = btl + R(2) * (mL[0] * b0[0] + mL[1] * b0[1] + mL[2] * b0[2]);
-    const R bsr = btr + R(2) * (mR[0] * b0[0] + mR[1] * b0[1] + mR[2] * b0[2]);
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-      const R pl = a == D ? R(0.5) * bsl : R(0), pr = a == D ? R(0.5) * bsr : R(0);
-      const R tl = R(0.5) * (pl - (mL[a] + b0[a]) * bn - mL[a] * b0[D]);
-      const R tr = R(0.5) * (pr - (mR[a] + b0[a]) * bn - mR[a] * b0[D]);
-      o[(6 + a) * fs] = (tl + tr) - bq * (Rt[V1 + a] - L[V1 + a]);
-    }
-  } else {
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-      R tl, tr;
-      if (a == D) {
-        tl = R(0.5) * (R(0.5) * btl - mL[a] * bn);
-        tr = R(0.5) * (R(0.5) * btr - mR[a] * bn);
-      } else {
-        tl = R(0.5) * (-mL[a] * bn);
-        tr = R(0.5) * (-mR[a] * bn);
-      }
-      o[(6 + a) * fs] = (tl + tr) - bq * (Rt[V1 + a] - L[V1 + a]);
-    }
-  }
-}
 
 // PDM reconstruction of the 9 face states, then flux_out: one thread per face
 // (PSL: the entropy channel p_S is live, Params::ps_live)
@@ -1338,6 +1206,7 @@ Tune::Tune() {
   blk[K_C2C2] = blk[K_EMF2] = blk[K_FLUX2] = dim3(32, 1, 8);
   // the first edge sweep of edges along j covers only the 8 ghost layers of i
   blk[K_C2C1] = dim3(8, 32, 1);
+  for (int d = 0; d < 3; d++) flux_sweep[d] = true;
 }
 
 dim3 launch_space(const Params& P, int slot) {
@@ -1403,7 +1272,8 @@ void launch_dt(const Params& P, int coord, bool mixed, cudaStream_t st) {
 
 template <typename R, bool BG>
 static void launch_slot_bg(const Params& P, int coord, const Work<R>& w, int slot, dim3 blk,
-                           cudaStream_t st) {
+                           cudaStream_t st, const SweepSet* sw) {
+  if (slot >= K_FLUX0 && slot <= K_FLUX2 && launch_flux_sweep<R>(sw, P, w, slot - K_FLUX0, st)) return;
   const dim3 sp = launch_space(P, slot);
   const dim3 g = grid3(sp.x, sp.y, sp.z, blk);
   switch (slot) {
@@ -1444,17 +1314,19 @@ static void launch_slot_bg(const Params& P, int coord, const Work<R>& w, int slo
 
 template <typename R>
 void launch_slot(const Params& P, int coord, const Work<R>& w, int slot, dim3 blk,
-                 cudaStream_t st) {
-  if (P.bg) launch_slot_bg<R, true>(P, coord, w, slot, blk, st);
-  else launch_slot_bg<R, false>(P, coord, w, slot, blk, st);
+                 cudaStream_t st, const SweepSet* sw) {
+  if (P.bg) launch_slot_bg<R, true>(P, coord, w, slot, blk, st, sw);
+  else launch_slot_bg<R, false>(P, coord, w, slot, blk, st, sw);
 }
 
-template void launch_slot<double>(const Params&, int, const Work<double>&, int, dim3, cudaStream_t);
-template void launch_slot<float>(const Params&, int, const Work<float>&, int, dim3, cudaStream_t);
+template void launch_slot<double>(const Params&, int, const Work<double>&, int, dim3, cudaStream_t,
+                                  const SweepSet*);
+template void launch_slot<float>(const Params&, int, const Work<float>&, int, dim3, cudaStream_t,
+                                 const SweepSet*);
 
 template <typename R>
 void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t st,
-                      const Tune& tune, const Hook& hook) {
+                      const Tune& tune, const SweepSet* sw, const Hook& hook) {
   hook(G_AB2, 1);
   launch_slot<R>(P, coord, w, K_AB2, tune.blk[K_AB2], st);
   hook(G_AB2, 0);
@@ -1464,7 +1336,8 @@ void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t
     hook(g, 1);
     for (int d = 0; d < 3; d++) {
       const int slot = K_C2C0 + 3 * stage + d;
-      launch_slot<R>(P, coord, w, slot, tune.blk[slot], st);
+      const SweepSet* use = stage == 2 && tune.flux_sweep[d] ? sw : nullptr;
+      launch_slot<R>(P, coord, w, slot, tune.blk[slot], st, use);
     }
     hook(g, 0);
   }
@@ -1486,9 +1359,9 @@ void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t
 }
 
 template void launch_step_body<double>(const Params&, int, const Work<double>&, cudaStream_t,
-                                       const Tune&, const Hook&);
+                                       const Tune&, const SweepSet*, const Hook&);
 template void launch_step_body<float>(const Params&, int, const Work<float>&, cudaStream_t,
-                                      const Tune&, const Hook&);
+                                      const Tune&, const SweepSet*, const Hook&);
 
 dim3 ghost_block(int slot) {
   if (slot == K_WRAP0) return dim3(8, 16, 2);               // 8 layers along i

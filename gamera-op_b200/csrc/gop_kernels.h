@@ -43,18 +43,34 @@ enum TuneSlot : int { K_AB2 = 0, K_C2C0, K_C2C1, K_C2C2, K_EMF0, K_EMF1, K_EMF2,
                       K_BC5, NSLOT };
 struct Tune {
   dim3 blk[NTUNE];
+  // flux of axis d from the tile-staged sweep kernel (gop_sweep.cu) instead
+  // of the per-face kernel, where the sweep applies
+  bool flux_sweep[3];
   Tune();
 };
+
+// Tensor maps and launch data of an instance's tile-staged flux sweeps
+// (gop_sweep.cu); null when they could not be made (the per-face kernels run)
+struct SweepSet;
+template <typename R>
+SweepSet* sweep_create(const Params& P, const Work<R>& w);
+void sweep_destroy(SweepSet* s);
+// the flux of axis D by the sweep kernel; false (nothing launched) where the
+// sweep does not apply (no maps, or the entropy channel is live)
+template <typename R>
+bool launch_flux_sweep(const SweepSet* sw, const Params& P, const Work<R>& w, int D,
+                       cudaStream_t st);
 
 // points covered by the launch of one slot (x, y, z extents)
 dim3 launch_space(const Params& P, int slot);
 // thread-block shape of a ghost-fill slot (K_WRAP*, K_BC*)
 dim3 ghost_block(int slot);
 
-// launches one tunable kernel alone (for the autotuner)
+// launches one tunable kernel alone (for the autotuner); a flux slot with
+// sw set runs the sweep kernel instead (blk unused)
 template <typename R>
 void launch_slot(const Params& P, int coord, const Work<R>& w, int slot, dim3 blk,
-                 cudaStream_t st);
+                 cudaStream_t st, const SweepSet* sw = nullptr);
 
 // optional timing hook: mark(ctx, group, start) records an event on the stream
 struct Hook {
@@ -75,7 +91,7 @@ void launch_dt(const Params& P, int coord, bool mixed, cudaStream_t st);
 void launch_ps_check(const Params& P, cudaStream_t st);
 template <typename R>
 void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t st,
-                      const Tune& tune, const Hook& hook = Hook());
+                      const Tune& tune, const SweepSet* sw, const Hook& hook = Hook());
 // which = 0: the buffer being written this step; 1: the current state
 void launch_ghosts(const Params& P, const char bc[6], const char gem_bc[6], int which,
                    cudaStream_t st);

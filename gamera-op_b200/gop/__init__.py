@@ -102,6 +102,7 @@ def lib():
         L.gop_background_init.argtypes = [C.POINTER(Desc), C.POINTER(Background), _dp, _dp, _dp, _dp]
         L.gop_autotune.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
         L.gop_set_profiling.argtypes = [vp, C.c_int]
+        L.gop_set_sweep.argtypes = [vp, C.c_int]
         L.gop_get_profile.argtypes = [vp, _dp, C.POINTER(C.c_int64)]
         L.gop_batch_create.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(vp)]
         L.gop_batch_destroy.argtypes = [vp]
@@ -288,6 +289,11 @@ class Instance:
         out = (C.c_int * len(self.TUNE_SLOTS))()
         _check(lib().gop_autotune(self._h, int(reps), out))
         return dict(zip(self.TUNE_SLOTS, list(out)))
+
+    def set_sweep(self, on: bool):
+        """Face fluxes by the tile-staged sweep kernels (default) or the
+        per-face kernels."""
+        _check(lib().gop_set_sweep(self._h, int(bool(on))))
 
     def set_profiling(self, on: bool):
         _check(lib().gop_set_profiling(self._h, int(bool(on))))

@@ -90,7 +90,8 @@ typedef struct {
   double dt0;        /* dt0 (previous dt, AB2 history) */
   double divb_max;   /* divB_max of the current state (src/solver_func.c:324-343) */
   int64_t steps;     /* steps taken since prepare */
-  int32_t flags;     /* nonzero: non-finite or non-positive state was seen */
+  int32_t flags;     /* 1: non-finite or non-positive state was seen;
+                        2: a device-side pipeline wait timed out */
   int32_t reserved;
   size_t device_bytes; /* device memory held by this instance */
 } gop_stats;
@@ -152,7 +153,16 @@ int gop_get_stats(gop_instance *h, gop_stats *out);
  * following steps.  reps: timed launches per candidate (0 = 3); chosen
  * (optional, 11 ints) receives the picked candidate index per launch. */
 #define GOP_NTUNE 11
+#define GOP_TUNE_SWEEP 14 /* chosen[] value of a flux launch: the tile-staged sweep kernel */
 int gop_autotune(gop_instance *h, int reps, int *chosen);
+
+/* Kernel choice for the face flux of each axis: on (the default) runs the
+ * tile-staged sweep kernels (shared-memory tiles filled by the Tensor Memory
+ * Accelerator, one persistent block per SM slot) wherever they apply, off
+ * the per-face kernels; both give the same results.  With the entropy
+ * channel live the per-face kernels always run.  GOP_ENODEV if the sweep
+ * kernels could not be set up for this instance. */
+int gop_set_sweep(gop_instance *h, int on);
 
 /* Diagnostics: time every kernel group of every step with CUDA events on
  * the instance's stream (off by default; switching resets the totals).
