@@ -1183,7 +1183,20 @@ static dim3 grid3(int a, int b, int c, dim3 blk) {
   return dim3((a + blk.x - 1) / blk.x, (b + blk.y - 1) / blk.y, (c + blk.z - 1) / blk.z);
 }
 
-#define LAUNCH(kern, grd, blk, st, ...)                                          \
+// 1: step kernels go out with programmatic dependent launch
+#ifndef GOP_PDL
+#define GOP_PDL 1
+#endif
+// 1: also the first kernel after the tile-staged flux sweeps.  Off: placed
+// early, its blocks (and the blocks launched early after them) start on SMs
+// still configured for the sweep's 213 KB of shared memory, with a short
+// L1, and the L1-bound edge-EMF stage slows down (blast 256^3 FP64 step
+// 9.49 vs 8.09 ms on B200)
+#ifndef GOP_PDL_AFTER_SWEEP
+#define GOP_PDL_AFTER_SWEEP 0
+#endif
+
+#define LAUNCH_PDL(pdl, kern, grd, blk, st, ...)                                 \
   do {                                                                           \
     cudaLaunchAttribute at_[1];                                                  \
     at_[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;              \
@@ -1193,10 +1206,11 @@ static dim3 grid3(int a, int b, int c, dim3 blk) {
     cfg_.blockDim = dim3(blk);                                                   \
     cfg_.stream = st;                                                            \
     cfg_.attrs = at_;                                                            \
-    cfg_.numAttrs = 1;                                                           \
+    cfg_.numAttrs = (GOP_PDL && (pdl)) ? 1 : 0;                                  \
     cudaLaunchKernelEx(&cfg_, kern, __VA_ARGS__);                                \
     g_launches++;                                                                \
   } while (0)
+#define LAUNCH(kern, grd, blk, st, ...) LAUNCH_PDL(true, kern, grd, blk, st, __VA_ARGS__)
 
 Tune::Tune() {
   // defaults: warps along i; the sweeps of D=1 / D=2 kernels run along the
@@ -1272,7 +1286,7 @@ void launch_dt(const Params& P, int coord, bool mixed, cudaStream_t st) {
 
 template <typename R, bool BG>
 static void launch_slot_bg(const Params& P, int coord, const Work<R>& w, int slot, dim3 blk,
-                           cudaStream_t st, const SweepSet* sw) {
+                           cudaStream_t st, const SweepSet* sw, bool pdl) {
   if (slot >= K_FLUX0 && slot <= K_FLUX2 && launch_flux_sweep<R>(sw, P, w, slot - K_FLUX0, st)) return;
   const dim3 sp = launch_space(P, slot);
   const dim3 g = grid3(sp.x, sp.y, sp.z, blk);
@@ -1281,7 +1295,7 @@ static void launch_slot_bg(const Params& P, int coord, const Work<R>& w, int slo
       if (P.ps_live) LAUNCH((k_ab2<R, true>), g, blk, st, P, w);
       else LAUNCH((k_ab2<R, false>), g, blk, st, P, w);
       break;
-    case K_C2C0: LAUNCH((k_c2c<R, 0>), g, blk, st, P, w); break;
+    case K_C2C0: LAUNCH_PDL(pdl, (k_c2c<R, 0>), g, blk, st, P, w); break;
     case K_C2C1: LAUNCH((k_c2c<R, 1>), g, blk, st, P, w); break;
     case K_C2C2: LAUNCH((k_c2c<R, 2>), g, blk, st, P, w); break;
     case K_EMF0: LAUNCH((k_emf<R, 0, BG>), g, blk, st, P, w); break;
@@ -1314,15 +1328,15 @@ static void launch_slot_bg(const Params& P, int coord, const Work<R>& w, int slo
 
 template <typename R>
 void launch_slot(const Params& P, int coord, const Work<R>& w, int slot, dim3 blk,
-                 cudaStream_t st, const SweepSet* sw) {
-  if (P.bg) launch_slot_bg<R, true>(P, coord, w, slot, blk, st, sw);
-  else launch_slot_bg<R, false>(P, coord, w, slot, blk, st, sw);
+                 cudaStream_t st, const SweepSet* sw, bool pdl) {
+  if (P.bg) launch_slot_bg<R, true>(P, coord, w, slot, blk, st, sw, pdl);
+  else launch_slot_bg<R, false>(P, coord, w, slot, blk, st, sw, pdl);
 }
 
 template void launch_slot<double>(const Params&, int, const Work<double>&, int, dim3, cudaStream_t,
-                                  const SweepSet*);
+                                  const SweepSet*, bool);
 template void launch_slot<float>(const Params&, int, const Work<float>&, int, dim3, cudaStream_t,
-                                 const SweepSet*);
+                                 const SweepSet*, bool);
 
 template <typename R>
 void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t st,
@@ -1337,7 +1351,11 @@ void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t
     for (int d = 0; d < 3; d++) {
       const int slot = K_C2C0 + 3 * stage + d;
       const SweepSet* use = stage == 2 && tune.flux_sweep[d] ? sw : nullptr;
-      launch_slot<R>(P, coord, w, slot, tune.blk[slot], st, use);
+      // the launch after a persistent sweep grid waits for it to finish
+      // instead of being placed early on SMs still configured for the
+      // sweep's shared memory (and its short L1)
+      const bool pdl = !(stage == 0 && d == 0 && sw && tune.flux_sweep[2]) || GOP_PDL_AFTER_SWEEP;
+      launch_slot<R>(P, coord, w, slot, tune.blk[slot], st, use, pdl);
     }
     hook(g, 0);
   }

@@ -67,10 +67,11 @@ dim3 launch_space(const Params& P, int slot);
 dim3 ghost_block(int slot);
 
 // launches one tunable kernel alone (for the autotuner); a flux slot with
-// sw set runs the sweep kernel instead (blk unused)
+// sw set runs the sweep kernel instead (blk unused); pdl false: without
+// programmatic dependent launch
 template <typename R>
 void launch_slot(const Params& P, int coord, const Work<R>& w, int slot, dim3 blk,
-                 cudaStream_t st, const SweepSet* sw = nullptr);
+                 cudaStream_t st, const SweepSet* sw = nullptr, bool pdl = true);
 
 // optional timing hook: mark(ctx, group, start) records an event on the stream
 struct Hook {

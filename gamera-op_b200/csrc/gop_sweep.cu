@@ -51,10 +51,29 @@ constexpr int kSweepThreads = 32 * kConsumerWarps;
 
 // shared-memory ring and residency per arithmetic type: two 53 KB slots
 // and two blocks per SM in FP64, two 26 KB slots and three blocks in FP32
+#ifndef GOP_SWEEP_STAGES_F64
+#define GOP_SWEEP_STAGES_F64 2
+#endif
+#ifndef GOP_SWEEP_STAGES_F32
+#define GOP_SWEEP_STAGES_F32 2
+#endif
+#ifndef GOP_SWEEP_CTAS_F64
+#define GOP_SWEEP_CTAS_F64 2
+#endif
+#ifndef GOP_SWEEP_CTAS_F32
+#define GOP_SWEEP_CTAS_F32 3
+#endif
+// 1: the sweeps go out with programmatic dependent launch like the other
+// step kernels.  Off: a sweep grid placed early onto SMs that still run the
+// previous kernel (persistent blocks, no room to spare) measured 2-20 %
+// slower on B200 (blast 256^3: FP32 flux 2.47 vs 2.06 ms per step)
+#ifndef GOP_SWEEP_PDL
+#define GOP_SWEEP_PDL 0
+#endif
 template <typename R>
 struct SweepCfg {
-  static constexpr int STAGES = 2;
-  static constexpr int CTAS = sizeof(R) == 8 ? 2 : 3;
+  static constexpr int STAGES = sizeof(R) == 8 ? GOP_SWEEP_STAGES_F64 : GOP_SWEEP_STAGES_F32;
+  static constexpr int CTAS = sizeof(R) == 8 ? GOP_SWEEP_CTAS_F64 : GOP_SWEEP_CTAS_F32;
 };
 
 template <int D>
@@ -97,7 +116,8 @@ static_assert(slots_aligned<double, 0>() && slots_aligned<double, 1>() && slots_
               "FP64 slot layout");
 static_assert(slots_aligned<float, 0>() && slots_aligned<float, 1>() && slots_aligned<float, 2>(),
               "FP32 slot layout");
-static_assert(sweep_smem<double, 1>() * 2 <= 227 * 1024, "two FP64 blocks per SM");
+static_assert(sweep_smem<double, 1>() * SweepCfg<double>::CTAS <= 228 * 1024, "FP64 blocks per SM");
+static_assert(sweep_smem<float, 1>() * SweepCfg<float>::CTAS <= 228 * 1024, "FP32 blocks per SM");
 
 struct alignas(64) FluxMaps {
   CUtensorMap wh;     // W_h, stencil box
@@ -398,7 +418,7 @@ static void launch_sweep_d(const SweepSet* sw, const Params& P, const Work<R>& w
   cfg.dynamicSmemBytes = sweep_smem<R, D>();
   cfg.stream = st;
   cfg.attrs = at;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = GOP_SWEEP_PDL ? 1 : 0;
   cudaLaunchKernelEx(&cfg, k_flux_sweep<R, D, BG>, P, w, m);
   count_launches(1);
 }

@@ -62,7 +62,7 @@ CASES = [
     dict(id="blast_32_fp64", n=(32, 32, 32), dom=(-0.5, 0.5) * 3, coord=0, bc="pppppp",
          kind="blast", prec=0, steps=20),
     dict(id="blast_ragged_77x45x21_bcmix", n=(77, 45, 21), dom=(-0.5, 0.5) * 3, coord=0,
-         bc="srfeep", kind="blast", prec=0, steps=12),
+         bc="srfepp", kind="blast", prec=0, steps=12),
     dict(id="ot_thin_64x64x4", n=(64, 64, 4), dom=(0, 1, 0, 1, 0, 1 / 64), coord=0, bc="pppppp",
          kind="ot", prec=0, steps=30),
     dict(id="sphere_67x35x19", n=(67, 35, 19),
