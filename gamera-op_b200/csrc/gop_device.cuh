@@ -257,6 +257,34 @@ __device__ __forceinline__ void pdm_pair(const R v[8], const R lim[4], const Fac
   }
 }
 
+// the same from a record in shared memory (16-byte aligned; the whole warp
+// reads one record)
+__device__ __forceinline__ void load_fw_smem(const float* rec, FaceWeights<float>& W) {
+  const float4* p = reinterpret_cast<const float4*>(rec);
+  const float4 a = p[0], b = p[1], c = p[2], d = p[3], e = p[4];
+  W.wl[0] = a.x; W.wl[1] = a.y; W.wl[2] = a.z; W.wl[3] = a.w;
+  W.wl[4] = b.x; W.wl[5] = b.y; W.wl[6] = b.z; W.wr[0] = b.w;
+  W.wr[1] = c.x; W.wr[2] = c.y; W.wr[3] = c.z; W.wr[4] = c.w;
+  W.wr[5] = d.x; W.wr[6] = d.y; W.cl1 = d.z; W.cl2 = d.w;
+  W.cr1 = e.x; W.cr2 = e.y;
+}
+__device__ __forceinline__ void load_fw_smem(const double* rec, FaceWeights<double>& W) {
+  const double2* p = reinterpret_cast<const double2*>(rec);
+  double v[18];
+#pragma unroll
+  for (int t = 0; t < 9; t++) {
+    const double2 q = p[t];
+    v[2 * t] = q.x;
+    v[2 * t + 1] = q.y;
+  }
+#pragma unroll
+  for (int t = 0; t < 7; t++) {
+    W.wl[t] = v[t];
+    W.wr[t] = v[7 + t];
+  }
+  W.cl1 = v[14]; W.cl2 = v[15]; W.cr1 = v[16]; W.cr2 = v[17];
+}
+
 // one face on its own: the three differences of lim computed here
 template <typename R>
 __device__ __forceinline__ void recon_lr(const R v[8], const R lim[4], const FaceWeights<R>& W,

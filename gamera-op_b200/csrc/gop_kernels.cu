@@ -366,7 +366,7 @@ __device__ __forceinline__ void flux_body(const Params& P, const Work<R>& wk, Po
     for (int u = 0; u < 4; u++) lim[u] = ms[(u - 2) * s];
     recon_lr<R>(v, lim, Wt, a1h, a2, mL[a], mR[a]);
   }
-  flux_out<R, D, BG, PSL>(P, wk, x, L, Rt, mL, mR);
+  flux_out<R, D, BG, PSL>(P, wk, x, L, Rt, mL, mR, lim_b<R>(P, wk)[x + D * fs]);
 }
 
 // --------------------------------------------------------------- update

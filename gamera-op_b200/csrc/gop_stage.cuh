@@ -41,13 +41,14 @@ __device__ __forceinline__ const R* lim_b(const Params& P, const Work<R>& wk) {
 }
 
 // Rusanov hydro flux and Maxwell stress at the face normal to D at cell x
-// from the reconstructed states (src/solver_func.c:934-1529).  F[9] =
-// mass, 3 momenta, energy, entropy, 3 stress components.  Also writes the
-// first centre-to-edge sweep of edges along (D+2)%3 (see c2c_body).
+// from the reconstructed states (src/solver_func.c:934-1529) and bn, the
+// step-start face field normal to the face.  F[9] = mass, 3 momenta,
+// energy, entropy, 3 stress components.  Also writes the first
+// centre-to-edge sweep of edges along (D+2)%3 (see c2c_body).
 template <typename R, int D, bool BG, bool PSL>
 __device__ __forceinline__ void flux_out(const Params& P, const Work<R>& wk, long long x,
                                          const R L[6], const R Rt[6], const R mL[3],
-                                         const R mR[3]) {
+                                         const R mR[3], const R bn) {
   const size_t fs = P.fs;
   // background field averaged over this face (B0Aface*_b1..3; the normal
   // component is B0Aface*_bn)
@@ -117,7 +118,6 @@ __device__ __forceinline__ void flux_out(const Params& P, const Work<R>& wk, lon
     fS = R(0.5) * (Sl * vnl + Sr * vnr - vfe * (Sr - Sl));
   }
   if constexpr (PSL) o[5 * fs] = fS;  // else the update takes a zero divergence
-  const R bn = lim_b<R>(P, wk)[x + D * fs];
   const R bq = (ttl + ttr) * (R)P.q_ca;
   if constexpr (BG) {
     // stress of B^2 + 2 B.B0 with the B0 cross terms

@@ -87,12 +87,19 @@ struct FluxTile {
   static constexpr int SB = SX * SY * SZ;  // elements per field, stencil box
   static constexpr int LB = LX * LY * LZ;  // elements per field, limiter box
   static constexpr int NG = 5;             // gas fields (the entropy channel is off)
-  // slot layout in elements of R: W_h, limiter W, mags_h, mags
+  // PDM weights of the tile's faces: D = 0 the 18 tap-major tables of the
+  // 32 faces (box (32, 18) of the per-axis tables), else the 8 packed face
+  // records (box (FW, 8))
+  static constexpr int WB = D == 0 ? 18 * 32 : FW * 8;
+  static constexpr int BNB = 256;          // step-start face field normal to the faces
+  // slot layout in elements of R: W_h, limiter W, mags_h, mags, weights, B_n
   static constexpr int OFF_WH = 0;
   static constexpr int OFF_WL = OFF_WH + NG * SB;
   static constexpr int OFF_MSH = OFF_WL + NG * LB;
   static constexpr int OFF_MS = OFF_MSH + 3 * SB;
-  static constexpr int ELEMS = OFF_MS + 3 * LB;
+  static constexpr int OFF_W = OFF_MS + 3 * LB;
+  static constexpr int OFF_BN = OFF_W + WB;
+  static constexpr int ELEMS = OFF_BN + BNB;
 };
 
 template <typename R, int D>
@@ -110,7 +117,7 @@ constexpr bool slots_aligned() {
   using T = FluxTile<D>;
   constexpr int e = sizeof(R);
   return (T::OFF_WL * e) % 128 == 0 && (T::OFF_MSH * e) % 128 == 0 && (T::OFF_MS * e) % 128 == 0 &&
-         (T::ELEMS * e) % 128 == 0;
+         (T::OFF_W * e) % 128 == 0 && (T::OFF_BN * e) % 128 == 0 && (T::ELEMS * e) % 128 == 0;
 }
 static_assert(slots_aligned<double, 0>() && slots_aligned<double, 1>() && slots_aligned<double, 2>(),
               "FP64 slot layout");
@@ -124,6 +131,8 @@ struct alignas(64) FluxMaps {
   CUtensorMap wl[2];  // limiter reference: FP64 the state buffer of each parity, FP32 its copy
   CUtensorMap msh;    // mags_h, stencil box
   CUtensorMap ms;     // mags, limiter box
+  CUtensorMap wt;     // PDM weights of the tile's faces
+  CUtensorMap bn[2];  // step-start face field (as wl: per parity in FP64)
   int nt[3];          // tiles: x, along the sweep (D = 0: rows of j), third axis
 };
 
@@ -184,7 +193,6 @@ __device__ __forceinline__ void flux_tile(const Params& P, const Work<R>& wk, co
   const bool on = T.i < NGH + P.n[0] + (D == 0) && T.j < NGH + P.n[1] + (D == 1) &&
                   T.k < NGH + P.n[2] + (D == 2);
   if (!on) return;
-  const int f = D == 0 ? T.i : (D == 1 ? T.j : T.k);
   // per-thread bases: tap t of field m is then at a compile-time offset
   const R* wh;
   const R* wl;
@@ -205,7 +213,21 @@ __device__ __forceinline__ void flux_tile(const Params& P, const Work<R>& wk, co
   }
   constexpr int TS = D == 0 ? 1 : 32;  // stride of one stencil tap in the slot
   FaceWeights<R> Wt;
-  load_face_weights<D, R>(wk.tab, wk.fw, P.tmax, f, Wt);
+  if constexpr (D == 0) {  // this lane's face in the 18 tap-major rows
+    const R* w = s + F::OFF_W + lane;
+#pragma unroll
+    for (int t = 0; t < 7; t++) {
+      Wt.wl[t] = w[t * 32];
+      Wt.wr[t] = w[(7 + t) * 32];
+    }
+    Wt.cl1 = w[14 * 32];
+    Wt.cl2 = w[15 * 32];
+    Wt.cr1 = w[16 * 32];
+    Wt.cr2 = w[17 * 32];
+  } else {  // the warp's face record (one broadcast address)
+    load_fw_smem(s + F::OFF_W + warp * FW, Wt);
+  }
+  const R bn = s[F::OFF_BN + warp * 32 + lane];
   const R a1h = (R)(0.5 * P.pdm_a1), a2 = (R)P.pdm_a2;
   R L[6], Rt[6], mL[3], mR[3];
   L[PS] = Rt[PS] = R(0);
@@ -227,7 +249,7 @@ __device__ __forceinline__ void flux_tile(const Params& P, const Work<R>& wk, co
     for (int u = 0; u < 4; u++) lim[u] = ms[a * F::LB + u * TS];
     recon_lr<R>(v, lim, Wt, a1h, a2, mL[a], mR[a]);
   }
-  flux_out<R, D, BG, false>(P, wk, lin(P, T.i, T.j, T.k), L, Rt, mL, mR);
+  flux_out<R, D, BG, false>(P, wk, lin(P, T.i, T.j, T.k), L, Rt, mL, mR, bn);
 }
 
 // Persistent flux sweep along D (entropy channel off).  Lane 0 of warp 0
@@ -253,7 +275,9 @@ __global__ void __launch_bounds__(kSweepThreads, SweepCfg<R>::CTAS)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const bool feeder = threadIdx.x == 0;
   const int ntiles = maps.nt[0] * maps.nt[1] * maps.nt[2];
-  const CUtensorMap* wl = &maps.wl[sizeof(R) == 8 ? cur_buf(P) : 0];
+  const int par = sizeof(R) == 8 ? cur_buf(P) : 0;
+  const CUtensorMap* wl = &maps.wl[par];
+  const CUtensorMap* bnm = &maps.bn[par];
   // issues the copies of the n-th tile of this block (tile index t) into its slot
   auto issue = [&](int n, int t) {
     const int q = n % S;
@@ -264,6 +288,15 @@ __global__ void __launch_bounds__(kSweepThreads, SweepCfg<R>::CTAS)
     tma_load_4d(s + F::OFF_WL, wl, &full[q], T.sx, T.ly, T.lz, 0);
     tma_load_4d(s + F::OFF_MSH, &maps.msh, &full[q], T.sx, T.sy, T.sz, 0);
     tma_load_4d(s + F::OFF_MS, &maps.ms, &full[q], T.sx, T.ly, T.lz, 0);
+    // weights: D = 0 rows T_WL0.. of the faces f0..f0+31 of axis 0; else the
+    // records of faces f0..f0+7 of axis D
+    const int f0 = D == 0 ? T.sx + NGH : (D == 1 ? T.sy + NGH : T.sz + NGH);
+    if constexpr (D == 0) tma_load_4d(s + F::OFF_W, &maps.wt, &full[q], f0, T_WL0, 0, 0);
+    else tma_load_4d(s + F::OFF_W, &maps.wt, &full[q], 0, D * P.tmax + f0, 0, 0);
+    // B_n at the tile's faces
+    if constexpr (D == 0) tma_load_4d(s + F::OFF_BN, bnm, &full[q], f0, T.sy, T.sz, 0);
+    else if constexpr (D == 1) tma_load_4d(s + F::OFF_BN, bnm, &full[q], T.sx, f0, T.sz, 1);
+    else tma_load_4d(s + F::OFF_BN, bnm, &full[q], T.sx, T.sy, f0, 2);
   };
   int issued = 0;  // feeder only: tiles whose copies were issued
   if (feeder) {
@@ -347,15 +380,47 @@ static bool make_map(CUtensorMap* m, const R* base, int nf, const Params& P, int
   return r == CUDA_SUCCESS;
 }
 
+// a 4-D map over a plain array of dims d[0..3] (elements, d[0] fastest)
+template <typename R>
+static bool make_map_dims(CUtensorMap* m, const R* base, const cuuint64_t d[4], const int box[4]) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn || !base) return false;
+  const cuuint64_t es = sizeof(R);
+  const cuuint64_t strides[3] = {d[0] * es, d[0] * d[1] * es, d[0] * d[1] * d[2] * es};
+  const cuuint32_t bx[4] = {(cuuint32_t)box[0], (cuuint32_t)box[1], (cuuint32_t)box[2], (cuuint32_t)box[3]};
+  const cuuint32_t el[4] = {1, 1, 1, 1};
+  const CUresult r =
+      fn(m, sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+         const_cast<R*>(base), d, strides, bx, el, CU_TENSOR_MAP_INTERLEAVE_NONE,
+         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
 template <typename R, int D>
 static bool make_flux_maps(FluxMaps& m, const Params& P, const Work<R>& w) {
   using F = FluxTile<D>;
   bool ok = make_map<R>(&m.wh, w.Wh, 6, P, F::SX, F::SY, F::SZ, F::NG) &&
             make_map<R>(&m.msh, w.Msh, 3, P, F::SX, F::SY, F::SZ, 3) &&
             make_map<R>(&m.ms, w.Ms, 3, P, F::LX, F::LY, F::LZ, 3);
+  // face field normal to the faces: box (32, 8, 1), (32, 8, 1) or (32, 1, 8)
+  const int bx = 32, by = D == 2 ? 1 : 8, bz = D == 2 ? 8 : 1;
   for (int b = 0; b < 2 && ok; b++) {
     const R* lim = sizeof(R) == 8 ? reinterpret_cast<const R*>(P.Wbuf[b]) : w.Wl;
-    ok = make_map<R>(&m.wl[b], lim, 6, P, F::LX, F::LY, F::LZ, F::NG);
+    const R* fb = sizeof(R) == 8 ? reinterpret_cast<const R*>(P.Bbuf[b]) : w.Bl;
+    ok = make_map<R>(&m.wl[b], lim, 6, P, F::LX, F::LY, F::LZ, F::NG) &&
+         make_map<R>(&m.bn[b], fb, 3, P, bx, by, bz, 1);
+  }
+  if (ok) {
+    const cuuint64_t tm = (cuuint64_t)P.tmax;
+    if (D == 0) {  // the per-axis tables [axis][NTAB][tmax]
+      const cuuint64_t d[4] = {tm, (cuuint64_t)NTAB, 3, 1};
+      const int box[4] = {32, 18, 1, 1};
+      ok = make_map_dims<R>(&m.wt, w.tab, d, box);
+    } else {       // the packed face records [axis * tmax + f][FW]
+      const cuuint64_t d[4] = {(cuuint64_t)FW, 3 * tm, 1, 1};
+      const int box[4] = {FW, 8, 1, 1};
+      ok = make_map_dims<R>(&m.wt, w.fw, d, box);
+    }
   }
   const int n0 = P.n[0], n1 = P.n[1], n2 = P.n[2];
   if (D == 0) {
