@@ -607,6 +607,11 @@ int gop_create(const gop_desc* desc, gop_instance** out) {
   // the tile-staged flux sweeps read the work and state arrays through
   // tensor maps made once here; without them the per-face kernels run
   h->sweep = mixed ? sweep_create<float>(P, h->wf) : sweep_create<double>(P, h->wd);
+  // FP32 edge EMFs: the per-edge kernel measured faster on B200 (blast 256^3:
+  // 1.09 vs 1.26 ms per step), FP64 the sweep (2.06 vs 2.25 ms); the
+  // autotuner decides per launch
+  if (mixed)
+    for (int d = 0; d < 3; d++) h->tune.emf_sweep[d] = false;
   cudaError_t le = e != cudaSuccess ? e : cudaStreamSynchronize(h->st);
   if (le == cudaSuccess) le = cudaGetLastError();
   if (le != cudaSuccess) {
@@ -991,9 +996,11 @@ int gop_autotune(gop_instance* h, int reps, int* chosen) {
   for (int slot = 0; slot < NTUNE; slot++) {
     float best = 1e30f;
     int best_c = 0;
-    // the flux slots also try the tile-staged sweep kernel (candidate ncand)
+    // the flux and EMF slots also try the tile-staged sweep kernel
+    // (candidate ncand)
     const bool flux = slot >= K_FLUX0 && slot <= K_FLUX2;
-    const bool try_sweep = flux && h->sweep && !P.ps_live;
+    const bool emf = slot >= K_EMF0 && slot <= K_EMF2;
+    const bool try_sweep = h->sweep && (emf || (flux && !P.ps_live));
     for (int c = 0; c < ncand + (try_sweep ? 1 : 0); c++) {
       const bool sw = c == ncand;
       if (!sw && cand[c].x * cand[c].y * cand[c].z > 256) continue;
@@ -1015,6 +1022,7 @@ int gop_autotune(gop_instance* h, int reps, int* chosen) {
     }
     if (best_c < ncand) h->tune.blk[slot] = cand[best_c];
     if (flux) h->tune.flux_sweep[slot - K_FLUX0] = best_c == ncand;
+    if (emf) h->tune.emf_sweep[slot - K_EMF0] = best_c == ncand;
     if (chosen) chosen[slot] = best_c;
     drop_step_graph(h);  // the captured step has the old shapes
   }
@@ -1035,7 +1043,7 @@ int gop_set_sweep(gop_instance* h, int on) {
   if (!h) return fail(GOP_EINVAL, "instance is NULL");
   if (on && !h->sweep) return fail(GOP_ENODEV, "the tile-staged sweep kernels are not available");
   CK(cudaStreamSynchronize(h->st));
-  for (int d = 0; d < 3; d++) h->tune.flux_sweep[d] = on != 0;
+  for (int d = 0; d < 3; d++) h->tune.flux_sweep[d] = h->tune.emf_sweep[d] = on != 0;
   drop_step_graph(h);
   return GOP_OK;
 }

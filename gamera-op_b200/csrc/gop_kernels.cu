@@ -307,21 +307,16 @@ __device__ __forceinline__ void emf_body(const Params& P, const Work<R>& wk, Pos
     for (int u = 0; u < 4; u++) lim[u] = B[q * fs + (u - 2) * sp];
     recon_lr<R>(v, lim, Wt, a1h, a2, bql, bqr);
   }
-  R bp = R(0.5) * (bpl + bpr), bq = R(0.5) * (bql + bqr);
-  if constexpr (BG) {  // + B0 averaged along the edge (B0Aedge*)
-    bp += (R)P.bg[(size_t)(BG_EDGE + 3 * D + p) * fs + x];
-    bq += (R)P.bg[(size_t)(BG_EDGE + 3 * D + q) * fs + x];
+  R b0p = R(0), b0q = R(0);
+  if constexpr (BG) {  // B0 averaged along the edge (B0Aedge*)
+    b0p = (R)P.bg[(size_t)(BG_EDGE + 3 * D + p) * fs + x];
+    b0q = (R)P.bg[(size_t)(BG_EDGE + 3 * D + q) * fs + x];
   }
-  const R vp = vav[0], vq = vav[1];
-  R e = -(vp * bq - vq * bp);
   const R* rh = wk.Wh + x;  // density slot
   // the reference sums the four densities around the edge in (i,j,k) order
   const R rho4 = D == 1 ? rh[-sq - sp] + rh[-sq] + rh[-sp] + rh[0]
                         : rh[-sp - sq] + rh[-sp] + rh[-sq] + rh[0];
-  const R ca = (R)P.ca;
-  R vz = sqrt((bp * bp + bq * bq) / (R(0.25) * rho4));
-  vz = vz * ca * rsq(vz * vz + ca * ca) + sqrt(vp * vp + vq * vq);
-  e += R(0.5) * vz * (bpl + bqr - bpr - bql);
+  const R e = emf_finish<R, BG>(P, vav[0], vav[1], bpl, bpr, bql, bqr, b0p, b0q, rho4);
   wk.E[x + (size_t)D * fs] = e;
 }
 
@@ -1220,7 +1215,7 @@ Tune::Tune() {
   blk[K_C2C2] = blk[K_EMF2] = blk[K_FLUX2] = dim3(32, 1, 8);
   // the first edge sweep of edges along j covers only the 8 ghost layers of i
   blk[K_C2C1] = dim3(8, 32, 1);
-  for (int d = 0; d < 3; d++) flux_sweep[d] = true;
+  for (int d = 0; d < 3; d++) flux_sweep[d] = emf_sweep[d] = true;
 }
 
 dim3 launch_space(const Params& P, int slot) {
@@ -1288,6 +1283,7 @@ template <typename R, bool BG>
 static void launch_slot_bg(const Params& P, int coord, const Work<R>& w, int slot, dim3 blk,
                            cudaStream_t st, const SweepSet* sw, bool pdl) {
   if (slot >= K_FLUX0 && slot <= K_FLUX2 && launch_flux_sweep<R>(sw, P, w, slot - K_FLUX0, st)) return;
+  if (slot >= K_EMF0 && slot <= K_EMF2 && launch_emf_sweep<R>(sw, P, w, slot - K_EMF0, st)) return;
   const dim3 sp = launch_space(P, slot);
   const dim3 g = grid3(sp.x, sp.y, sp.z, blk);
   switch (slot) {
@@ -1315,11 +1311,11 @@ static void launch_slot_bg(const Params& P, int coord, const Work<R>& w, int slo
       break;
     case K_UPDATE:
       if (coord == 0) {
-        if (P.ps_live) LAUNCH((k_update<0, R, BG, true>), g, blk, st, P, w);
-        else LAUNCH((k_update<0, R, BG, false>), g, blk, st, P, w);
+        if (P.ps_live) LAUNCH_PDL(pdl, (k_update<0, R, BG, true>), g, blk, st, P, w);
+        else LAUNCH_PDL(pdl, (k_update<0, R, BG, false>), g, blk, st, P, w);
       } else {
-        if (P.ps_live) LAUNCH((k_update<2, R, BG, true>), g, blk, st, P, w);
-        else LAUNCH((k_update<2, R, BG, false>), g, blk, st, P, w);
+        if (P.ps_live) LAUNCH_PDL(pdl, (k_update<2, R, BG, true>), g, blk, st, P, w);
+        else LAUNCH_PDL(pdl, (k_update<2, R, BG, false>), g, blk, st, P, w);
       }
       break;
     default: break;
@@ -1350,22 +1346,24 @@ void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t
     hook(g, 1);
     for (int d = 0; d < 3; d++) {
       const int slot = K_C2C0 + 3 * stage + d;
-      const SweepSet* use = stage == 2 && tune.flux_sweep[d] ? sw : nullptr;
+      const bool sweep = sw && ((stage == 2 && tune.flux_sweep[d]) || (stage == 1 && tune.emf_sweep[d]));
       // the launch after a persistent sweep grid waits for it to finish
       // instead of being placed early on SMs still configured for the
       // sweep's shared memory (and its short L1)
       const bool pdl = !(stage == 0 && d == 0 && sw && tune.flux_sweep[2]) || GOP_PDL_AFTER_SWEEP;
-      launch_slot<R>(P, coord, w, slot, tune.blk[slot], st, use, pdl);
+      launch_slot<R>(P, coord, w, slot, tune.blk[slot], st, sweep ? sw : nullptr, pdl);
     }
     hook(g, 0);
   }
   hook(G_UPDATE, 1);
+  const bool after_emf_sweep = sw && tune.emf_sweep[2] && !GOP_PDL_AFTER_SWEEP;
   launch_pole_emf<R>(P, w, st);  // pole ring average only
   if (coord != 0) {  // curvilinear: the face fields in their own launch
     const dim3 blk = tune.blk[K_UPDATE];
-    LAUNCH((k_ct<2, R>), grid3(P.n[0], P.n[1], P.n[2], blk), blk, st, P, w);
+    LAUNCH_PDL(!after_emf_sweep, (k_ct<2, R>), grid3(P.n[0], P.n[1], P.n[2], blk), blk, st, P, w);
   }
-  launch_slot<R>(P, coord, w, K_UPDATE, tune.blk[K_UPDATE], st);
+  launch_slot<R>(P, coord, w, K_UPDATE, tune.blk[K_UPDATE], st, nullptr,
+                 coord != 0 || !after_emf_sweep);
   // the work arrays are free after the update: 2 fields of doubles of scratch
   if (P.ring) {
     launch_ring_average(P, reinterpret_cast<double*>(w.Wh), st);

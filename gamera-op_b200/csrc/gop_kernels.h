@@ -43,9 +43,11 @@ enum TuneSlot : int { K_AB2 = 0, K_C2C0, K_C2C1, K_C2C2, K_EMF0, K_EMF1, K_EMF2,
                       K_BC5, NSLOT };
 struct Tune {
   dim3 blk[NTUNE];
-  // flux of axis d from the tile-staged sweep kernel (gop_sweep.cu) instead
-  // of the per-face kernel, where the sweep applies
+  // flux of axis d / EMF of the edges along d from the tile-staged sweep
+  // kernels (gop_sweep.cu) instead of the per-point kernels, where the
+  // sweeps apply
   bool flux_sweep[3];
+  bool emf_sweep[3];
   Tune();
 };
 
@@ -60,15 +62,19 @@ void sweep_destroy(SweepSet* s);
 template <typename R>
 bool launch_flux_sweep(const SweepSet* sw, const Params& P, const Work<R>& w, int D,
                        cudaStream_t st);
+// the EMF of the edges along D by the sweep kernel; false without maps
+template <typename R>
+bool launch_emf_sweep(const SweepSet* sw, const Params& P, const Work<R>& w, int D,
+                      cudaStream_t st);
 
 // points covered by the launch of one slot (x, y, z extents)
 dim3 launch_space(const Params& P, int slot);
 // thread-block shape of a ghost-fill slot (K_WRAP*, K_BC*)
 dim3 ghost_block(int slot);
 
-// launches one tunable kernel alone (for the autotuner); a flux slot with
-// sw set runs the sweep kernel instead (blk unused); pdl false: without
-// programmatic dependent launch
+// launches one tunable kernel alone (for the autotuner); a flux or EMF slot
+// with sw set runs the sweep kernel instead (blk unused); pdl false:
+// without programmatic dependent launch
 template <typename R>
 void launch_slot(const Params& P, int coord, const Work<R>& w, int slot, dim3 blk,
                  cudaStream_t st, const SweepSet* sw = nullptr, bool pdl = true);

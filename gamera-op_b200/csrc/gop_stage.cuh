@@ -147,4 +147,24 @@ __device__ __forceinline__ void flux_out(const Params& P, const Work<R>& wk, lon
   }
 }
 
+// The edge EMF (src/solver_func.c:779-902) from the edge's reconstructions:
+// vp, vq the second-sweep velocities, (bpl, bpr) B_p reconstructed along q,
+// (bql, bqr) B_q along p, b0p / b0q the background field averaged along the
+// edge (BG), rho4 the sum of the four half-step densities around the edge.
+template <typename R, bool BG>
+__device__ __forceinline__ R emf_finish(const Params& P, R vp, R vq, R bpl, R bpr, R bql, R bqr,
+                                        R b0p, R b0q, R rho4) {
+  R bp = R(0.5) * (bpl + bpr), bq = R(0.5) * (bql + bqr);
+  if constexpr (BG) {
+    bp += b0p;
+    bq += b0q;
+  }
+  R e = -(vp * bq - vq * bp);
+  const R ca = (R)P.ca;
+  R vz = sqrt((bp * bp + bq * bq) / (R(0.25) * rho4));
+  vz = vz * ca * rsq(vz * vz + ca * ca) + sqrt(vp * vp + vq * vq);
+  e += R(0.5) * vz * (bpl + bqr - bpr - bql);
+  return e;
+}
+
 }  // namespace gop

@@ -1,40 +1,41 @@
-// Tile-staged flux sweeps of the MHD step for B200 (sm_100a).
+// Tile-staged sweeps of the MHD step for B200 (sm_100a): the face flux and
+// the edge EMF, the step's two stencil stages, computed from shared-memory
+// tiles that the Tensor Memory Accelerator streams in ahead of the
+// arithmetic.
 //
-// The face flux along axis D (PDM reconstruction of the 8 face states,
-// Rusanov flux and Maxwell stress, src/solver_func.c:215-253,503-685,
-// 934-1529) is the step's largest stage.  Its per-face form (k_flux in
-// gop_kernels.cu) gathers each face's 8-point stencils of 16 input fields
-// with ~100 global loads through L1; the loads' 64-bit address arithmetic
-// and their latency, not the FP64 arithmetic, bound it.  Here each block is
-// persistent and runs a copy pipeline:
+// Face flux along axis D: PDM reconstruction of the 8 face states, Rusanov
+// flux and Maxwell stress (src/solver_func.c:215-253,503-685,934-1529).
+// Edge EMF along axis D: the second centre-to-edge sweep, the two face-field
+// reconstructions and the EMF (src/solver_func.c:686-902).  Their per-point
+// forms (k_flux, k_emf in gop_kernels.cu) gather each output's 8-point
+// stencils with dozens of global loads through L1; the loads' 64-bit
+// address arithmetic and latency, not the FP64 arithmetic, bound them.
+// Here each block is persistent and runs a copy pipeline:
 //
 //   copies   one elected thread streams tiles into a ring of STAGES
 //            shared-memory slots with cp.async.bulk.tensor (one TMA box per
-//            input array and tile), completing on the slot's "full"
-//            mbarrier;
-//   compute  8 warps compute one face per thread from shared memory (every
-//            stencil tap is a load at a compile-time offset from one
-//            per-thread base) and release the slot on its "empty"
-//            mbarrier.
+//            input array and tile: stencil windows, limiter windows, PDM
+//            weights), completing on the slot's "full" mbarrier;
+//   compute  8 warps compute one face or edge per thread from shared memory
+//            (every stencil tap is a load at a compile-time offset from one
+//            per-thread base) and release the slot on its "empty" mbarrier;
+//            the feeding thread refills a released slot with the tile
+//            STAGES ahead.
 //
 // So the global-memory latency of tile n+1 overlaps the arithmetic of tile
 // n, and the stencil re-reads come from shared memory instead of L1.  The
-// per-face arithmetic is the per-face kernel's own (recon_lr, flux_out), in
-// the same order, so both kernels give the same results.
+// per-point arithmetic is the per-point kernels' own (recon_lr, flux_out,
+// emf_finish), in the same order, so both forms give the same bits.
 //
-// Tiles (x = i, y = j, z = k; one box per array, field extent nf):
-//   D = 0  32 faces along i (lanes) x 8 rows along j (warps) x 1 plane
-//          box (40, 8, 1) from (f0 - 4, j0, k): stencil and limiter alike
-//   D = 1  32 cells along i (lanes) x 8 faces along j (warps) x 1 plane
-//          stencil box (32, 15, 1) from (i0, f0 - 4, k),
-//          limiter box (32, 11, 1) from (i0, f0 - 2, k)
-//   D = 2  32 cells along i x 1 row x 8 faces along k (warps)
-//          stencil box (32, 1, 15) from (i0, j, f0 - 4),
-//          limiter box (32, 1, 11) from (i0, j, f0 - 2)
-// Every box starts at an x of f0 - 4 = 32 t or i0 = 4 + 32 t, so x times
-// the element size is a multiple of 16 bytes (the TMA's alignment rule).
-// Tiles are numbered with the x tile fastest, then the tile along the
-// sweep, so the blocks in flight at any time share their halo rows in L2.
+// Lanes always run along i (x, the TMA box's contiguous axis); a tile is 32
+// lanes x 8 warps, one warp per row along the stage's sweep axis or its
+// third axis.  Every box starts at an x of 32 t or 4 + 32 t, so x times the
+// element size is a multiple of 16 bytes (the TMA's alignment rule); no
+// coordinate is negative.  Boxes reaching past the grid are filled with
+// zeros by the TMA and only feed threads outside the grid, which store
+// nothing.  Tiles are numbered with the x tile fastest, then the tile along
+// the warps, so the blocks in flight at any time share their halo rows in
+// L2.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -46,11 +47,11 @@
 
 namespace gop {
 
-constexpr int kConsumerWarps = 8;
-constexpr int kSweepThreads = 32 * kConsumerWarps;
+constexpr int kWarps = 8;
+constexpr int kSweepThreads = 32 * kWarps;
 
-// shared-memory ring and residency per arithmetic type: two 53 KB slots
-// and two blocks per SM in FP64, two 26 KB slots and three blocks in FP32
+// shared-memory ring and residency per arithmetic type: two slots and two
+// blocks per SM in FP64 (128 registers), two slots and three blocks in FP32
 #ifndef GOP_SWEEP_STAGES_F64
 #define GOP_SWEEP_STAGES_F64 2
 #endif
@@ -76,55 +77,56 @@ struct SweepCfg {
   static constexpr int CTAS = sizeof(R) == 8 ? GOP_SWEEP_CTAS_F64 : GOP_SWEEP_CTAS_F32;
 };
 
+// a box of the slot: extents (x, y, z, fields) and elements, rounded up to
+// 32 so every box starts on a 128-byte boundary in FP32 and FP64
+struct Box {
+  int x, y, z, f;
+  __host__ __device__ constexpr int elems() const { return x * y * z * f; }
+  __host__ __device__ constexpr int padded() const { return (elems() + 31) / 32 * 32; }
+};
+constexpr Box kRec8{FW, 8, 1, 1};    // 8 packed face records
+constexpr Box kRec1{FW, 1, 1, 1};    // 1 packed face record
+constexpr Box kTap32{32, 18, 1, 1};  // tap-major weights of 32 faces (T_WL0..T_CR2)
+
+// weights of the 32 faces of one warp row (tap-major rows in shared memory)
+template <typename R>
+__device__ __forceinline__ void load_tap32(const R* w, FaceWeights<R>& W) {
+#pragma unroll
+  for (int u = 0; u < 7; u++) {
+    W.wl[u] = w[u * 32];
+    W.wr[u] = w[(7 + u) * 32];
+  }
+  W.cl1 = w[14 * 32];
+  W.cl2 = w[15 * 32];
+  W.cr1 = w[16 * 32];
+  W.cr2 = w[17 * 32];
+}
+
+// ------------------------------------------------------------------ flux
+
 template <int D>
 struct FluxTile {
-  static constexpr int SX = D == 0 ? 40 : 32;
-  static constexpr int SY = D == 0 ? 8 : (D == 1 ? 15 : 1);
-  static constexpr int SZ = D == 2 ? 15 : 1;
-  static constexpr int LX = SX;
-  static constexpr int LY = D == 1 ? 11 : SY;
-  static constexpr int LZ = D == 2 ? 11 : 1;
-  static constexpr int SB = SX * SY * SZ;  // elements per field, stencil box
-  static constexpr int LB = LX * LY * LZ;  // elements per field, limiter box
-  static constexpr int NG = 5;             // gas fields (the entropy channel is off)
-  // PDM weights of the tile's faces: D = 0 the 18 tap-major tables of the
-  // 32 faces (box (32, 18) of the per-axis tables), else the 8 packed face
-  // records (box (FW, 8))
-  static constexpr int WB = D == 0 ? 18 * 32 : FW * 8;
-  static constexpr int BNB = 256;          // step-start face field normal to the faces
-  // slot layout in elements of R: W_h, limiter W, mags_h, mags, weights, B_n
+  static constexpr int NG = 5;  // gas fields (the entropy channel is off)
+  // stencil and limiter windows of the tile's faces
+  static constexpr Box S = D == 0 ? Box{40, 8, 1, 1} : (D == 1 ? Box{32, 15, 1, 1} : Box{32, 1, 15, 1});
+  static constexpr Box L = D == 0 ? Box{40, 8, 1, 1} : (D == 1 ? Box{32, 11, 1, 1} : Box{32, 1, 11, 1});
+  static constexpr Box WT = D == 0 ? kTap32 : kRec8;
+  static constexpr Box BN = D == 2 ? Box{32, 1, 8, 1} : Box{32, 8, 1, 1};
+  static constexpr int SB = S.elems(), LB = L.elems();
+  // slot layout in elements: W_h, limiter W, mags_h, mags, weights, B_n
   static constexpr int OFF_WH = 0;
   static constexpr int OFF_WL = OFF_WH + NG * SB;
   static constexpr int OFF_MSH = OFF_WL + NG * LB;
   static constexpr int OFF_MS = OFF_MSH + 3 * SB;
   static constexpr int OFF_W = OFF_MS + 3 * LB;
-  static constexpr int OFF_BN = OFF_W + WB;
-  static constexpr int ELEMS = OFF_BN + BNB;
+  static constexpr int OFF_BN = OFF_W + WT.padded();
+  static constexpr int ELEMS = OFF_BN + BN.padded();
+  // elements the TMA delivers into a slot (the barrier's transaction count)
+  static constexpr int TX = NG * SB + NG * LB + 3 * SB + 3 * LB + WT.elems() + BN.elems();
+  static_assert((NG * SB) % 32 == 0 && (NG * LB) % 32 == 0 && (3 * SB) % 32 == 0 &&
+                    (3 * LB) % 32 == 0,
+                "flux boxes on 128-byte boundaries");
 };
-
-template <typename R, int D>
-__host__ __device__ constexpr int slot_bytes() {
-  return FluxTile<D>::ELEMS * (int)sizeof(R);
-}
-template <typename R, int D>
-__host__ __device__ constexpr int sweep_smem() {
-  return SweepCfg<R>::STAGES * slot_bytes<R, D>() + 2 * SweepCfg<R>::STAGES * 8 + 128;
-}
-
-// every TMA destination must start on a 128-byte boundary
-template <typename R, int D>
-constexpr bool slots_aligned() {
-  using T = FluxTile<D>;
-  constexpr int e = sizeof(R);
-  return (T::OFF_WL * e) % 128 == 0 && (T::OFF_MSH * e) % 128 == 0 && (T::OFF_MS * e) % 128 == 0 &&
-         (T::OFF_W * e) % 128 == 0 && (T::OFF_BN * e) % 128 == 0 && (T::ELEMS * e) % 128 == 0;
-}
-static_assert(slots_aligned<double, 0>() && slots_aligned<double, 1>() && slots_aligned<double, 2>(),
-              "FP64 slot layout");
-static_assert(slots_aligned<float, 0>() && slots_aligned<float, 1>() && slots_aligned<float, 2>(),
-              "FP32 slot layout");
-static_assert(sweep_smem<double, 1>() * SweepCfg<double>::CTAS <= 228 * 1024, "FP64 blocks per SM");
-static_assert(sweep_smem<float, 1>() * SweepCfg<float>::CTAS <= 228 * 1024, "FP32 blocks per SM");
 
 struct alignas(64) FluxMaps {
   CUtensorMap wh;     // W_h, stencil box
@@ -133,176 +135,341 @@ struct alignas(64) FluxMaps {
   CUtensorMap ms;     // mags, limiter box
   CUtensorMap wt;     // PDM weights of the tile's faces
   CUtensorMap bn[2];  // step-start face field (as wl: per parity in FP64)
-  int nt[3];          // tiles: x, along the sweep (D = 0: rows of j), third axis
+  int nt[3];          // tiles: x, along the warps, third axis
 };
 
-struct SweepSet {
-  FluxMaps flux[3];
-  int sms = 0;
-};
-
-// tile t of the sweep along D: TMA origin of the stencil and limiter boxes
-// and the cell / face of (warp, lane)
-template <int D>
+// tile t of the flux sweep along D: its first cell / face on each axis
 struct TileAt {
-  int sx, sy, sz;  // stencil box origin
-  int ly, lz;      // limiter box origin (x as the stencil's)
-  int i, j, k;     // this thread's face (index along D) and transverse cell
+  int x0, y0, z0;
 };
-
 template <int D>
-__device__ __forceinline__ TileAt<D> tile_at(const int nt[3], int t, int warp, int lane) {
+__device__ __forceinline__ TileAt flux_at(const int nt[3], int t) {
   const int a = t % nt[0], r = t / nt[0], b = r % nt[1], c = r / nt[1];
-  TileAt<D> T;
-  if constexpr (D == 0) {
-    T.sx = 32 * a;
-    T.sy = NGH + 8 * b;
-    T.sz = NGH + c;
-    T.ly = T.sy;
-    T.lz = T.sz;
-    T.i = NGH + 32 * a + lane;
-    T.j = NGH + 8 * b + warp;
-    T.k = NGH + c;
-  } else if constexpr (D == 1) {
-    T.sx = NGH + 32 * a;
-    T.sy = 8 * b;
-    T.sz = NGH + c;
-    T.ly = 8 * b + 2;
-    T.lz = T.sz;
-    T.i = NGH + 32 * a + lane;
-    T.j = NGH + 8 * b + warp;
-    T.k = NGH + c;
-  } else {
-    T.sx = NGH + 32 * a;
-    T.sy = NGH + c;
-    T.sz = 8 * b;
-    T.ly = T.sy;
-    T.lz = 8 * b + 2;
-    T.i = NGH + 32 * a + lane;
-    T.j = NGH + c;
-    T.k = NGH + 8 * b + warp;
+  TileAt T;
+  T.x0 = NGH + 32 * a;
+  if constexpr (D == 2) {  // warps: faces along k, one row j
+    T.y0 = NGH + c;
+    T.z0 = NGH + 8 * b;
+  } else {  // warps: rows along j (D = 0) or faces along j (D = 1), one plane k
+    T.y0 = NGH + 8 * b;
+    T.z0 = NGH + c;
   }
   return T;
 }
 
-// the faces of one tile from a filled slot (one face per consumer thread)
 template <typename R, int D, bool BG>
-__device__ __forceinline__ void flux_tile(const Params& P, const Work<R>& wk, const R* __restrict__ s,
-                                          const TileAt<D>& T, int warp, int lane) {
+struct FluxStage {
   using F = FluxTile<D>;
-  const bool on = T.i < NGH + P.n[0] + (D == 0) && T.j < NGH + P.n[1] + (D == 1) &&
-                  T.k < NGH + P.n[2] + (D == 2);
-  if (!on) return;
-  // per-thread bases: tap t of field m is then at a compile-time offset
-  const R* wh;
-  const R* wl;
-  const R* msh;
-  const R* ms;
-  if constexpr (D == 0) {
-    const int b = warp * F::SX + lane;
-    wh = s + F::OFF_WH + b;
-    wl = s + F::OFF_WL + b + 2;  // the limiter cells f-2..f+1 start 2 cells in
-    msh = s + F::OFF_MSH + b;
-    ms = s + F::OFF_MS + b + 2;
-  } else {
-    const int b = warp * 32 + lane;
-    wh = s + F::OFF_WH + b;
-    wl = s + F::OFF_WL + b;
-    msh = s + F::OFF_MSH + b;
-    ms = s + F::OFF_MS + b;
+  using Maps = FluxMaps;
+  static constexpr int ELEMS = F::ELEMS;
+  static constexpr int TX = F::TX;
+
+  __device__ static void issue(const Params& P, const Maps& m, int par, int t, R* s, uint64_t* bar) {
+    const TileAt T = flux_at<D>(m.nt, t);
+    const int f0 = D == 0 ? T.x0 : (D == 1 ? T.y0 : T.z0);  // first face along D
+    // stencil windows start 4 cells before the first face, limiter windows
+    // 2 (along i both start 4 before, keeping x aligned)
+    const int sx = D == 0 ? T.x0 - 4 : T.x0, sy = D == 1 ? T.y0 - 4 : T.y0, sz = D == 2 ? T.z0 - 4 : T.z0;
+    const int ly = D == 1 ? T.y0 - 2 : T.y0, lz = D == 2 ? T.z0 - 2 : T.z0;
+    tma_load_4d(s + F::OFF_WH, &m.wh, bar, sx, sy, sz, 0);
+    tma_load_4d(s + F::OFF_WL, &m.wl[par], bar, sx, ly, lz, 0);
+    tma_load_4d(s + F::OFF_MSH, &m.msh, bar, sx, sy, sz, 0);
+    tma_load_4d(s + F::OFF_MS, &m.ms, bar, sx, ly, lz, 0);
+    if constexpr (D == 0) tma_load_4d(s + F::OFF_W, &m.wt, bar, f0, T_WL0, 0, 0);
+    else tma_load_4d(s + F::OFF_W, &m.wt, bar, 0, D * P.tmax + f0, 0, 0);
+    tma_load_4d(s + F::OFF_BN, &m.bn[par], bar, T.x0, T.y0, T.z0, D);
   }
-  constexpr int TS = D == 0 ? 1 : 32;  // stride of one stencil tap in the slot
-  FaceWeights<R> Wt;
-  if constexpr (D == 0) {  // this lane's face in the 18 tap-major rows
-    const R* w = s + F::OFF_W + lane;
-#pragma unroll
-    for (int t = 0; t < 7; t++) {
-      Wt.wl[t] = w[t * 32];
-      Wt.wr[t] = w[(7 + t) * 32];
+
+  // one face per thread
+  __device__ static void compute(const Params& P, const Work<R>& wk, const Maps& m, const R* s,
+                                 int t, int warp, int lane) {
+    const TileAt T = flux_at<D>(m.nt, t);
+    const int i = T.x0 + lane, j = T.y0 + (D == 2 ? 0 : warp), k = T.z0 + (D == 2 ? warp : 0);
+    if (!(i < NGH + P.n[0] + (D == 0) && j < NGH + P.n[1] + (D == 1) && k < NGH + P.n[2] + (D == 2)))
+      return;
+    // per-thread bases: tap u of field f is then at a compile-time offset
+    const R *wh, *wl, *msh, *ms;
+    if constexpr (D == 0) {
+      const int b = warp * 40 + lane;
+      wh = s + F::OFF_WH + b;
+      wl = s + F::OFF_WL + b + 2;  // the limiter cells f-2..f+1 start 2 cells in
+      msh = s + F::OFF_MSH + b;
+      ms = s + F::OFF_MS + b + 2;
+    } else {
+      const int b = warp * 32 + lane;
+      wh = s + F::OFF_WH + b;
+      wl = s + F::OFF_WL + b;
+      msh = s + F::OFF_MSH + b;
+      ms = s + F::OFF_MS + b;
     }
-    Wt.cl1 = w[14 * 32];
-    Wt.cl2 = w[15 * 32];
-    Wt.cr1 = w[16 * 32];
-    Wt.cr2 = w[17 * 32];
-  } else {  // the warp's face record (one broadcast address)
-    load_fw_smem(s + F::OFF_W + warp * FW, Wt);
+    constexpr int TS = D == 0 ? 1 : 32;  // stride of one stencil tap in the slot
+    FaceWeights<R> Wt;
+    if constexpr (D == 0) load_tap32(s + F::OFF_W + lane, Wt);
+    else load_fw_smem(s + F::OFF_W + warp * FW, Wt);
+    const R bn = s[F::OFF_BN + warp * 32 + lane];
+    const R a1h = (R)(0.5 * P.pdm_a1), a2 = (R)P.pdm_a2;
+    R L[6], Rt[6], mL[3], mR[3];
+    L[PS] = Rt[PS] = R(0);
+#pragma unroll
+    for (int f = 0; f < F::NG; f++) {
+      R v[8], lim[4];
+#pragma unroll
+      for (int u = 0; u < 8; u++) v[u] = wh[f * F::SB + u * TS];
+#pragma unroll
+      for (int u = 0; u < 4; u++) lim[u] = wl[f * F::LB + u * TS];
+      recon_lr<R>(v, lim, Wt, a1h, a2, L[f], Rt[f]);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      R v[8], lim[4];
+#pragma unroll
+      for (int u = 0; u < 8; u++) v[u] = msh[a * F::SB + u * TS];
+#pragma unroll
+      for (int u = 0; u < 4; u++) lim[u] = ms[a * F::LB + u * TS];
+      recon_lr<R>(v, lim, Wt, a1h, a2, mL[a], mR[a]);
+    }
+    flux_out<R, D, BG, false>(P, wk, lin(P, i, j, k), L, Rt, mL, mR, bn);
   }
-  const R bn = s[F::OFF_BN + warp * 32 + lane];
-  const R a1h = (R)(0.5 * P.pdm_a1), a2 = (R)P.pdm_a2;
-  R L[6], Rt[6], mL[3], mR[3];
-  L[PS] = Rt[PS] = R(0);
-#pragma unroll
-  for (int m = 0; m < F::NG; m++) {
-    R v[8], lim[4];
-#pragma unroll
-    for (int t = 0; t < 8; t++) v[t] = wh[m * F::SB + t * TS];
-#pragma unroll
-    for (int u = 0; u < 4; u++) lim[u] = wl[m * F::LB + u * TS];
-    recon_lr<R>(v, lim, Wt, a1h, a2, L[m], Rt[m]);
+};
+
+// ------------------------------------------------------------------- EMF
+
+// Edge EMF along D, p = D+1, q = D+2 (mod 3).  Inputs per edge: the two
+// first-sweep velocities along q (V, 8 cells; limited against themselves),
+// B_p along q (8 half-step, 4 step-start values), B_q along p (8 + 4), the
+// four half-step densities around the edge, the weights of its q and p faces.
+//   D = 0 (p = j, q = k): lanes cells along i, warps k faces, one j face
+//   D = 1 (p = k, q = i): lanes i faces, warps k faces, one j cell
+//   D = 2 (p = i, q = j): lanes i faces, warps j faces, one k cell
+template <int D>
+struct EmfTile {
+  static constexpr Box V = D == 0 ? Box{32, 1, 15, 2} : (D == 1 ? Box{40, 1, 8, 2} : Box{32, 15, 1, 2});
+  static constexpr Box BHP = D == 0 ? Box{32, 1, 15, 1} : (D == 1 ? Box{40, 1, 8, 1} : Box{32, 15, 1, 1});
+  static constexpr Box BLP = D == 0 ? Box{32, 1, 11, 1} : (D == 1 ? Box{40, 1, 8, 1} : Box{32, 11, 1, 1});
+  static constexpr Box BHQ = D == 0 ? Box{32, 8, 8, 1} : (D == 1 ? Box{32, 1, 15, 1} : Box{40, 8, 1, 1});
+  static constexpr Box BLQ = D == 0 ? Box{32, 4, 8, 1} : (D == 1 ? Box{32, 1, 11, 1} : Box{40, 8, 1, 1});
+  static constexpr Box RHO = D == 0 ? Box{32, 2, 9, 1} : (D == 1 ? Box{40, 1, 9, 1} : Box{40, 9, 1, 1});
+  static constexpr Box WQ = D == 1 ? kTap32 : kRec8;
+  static constexpr Box WP = D == 0 ? kRec1 : (D == 1 ? kRec8 : kTap32);
+  static constexpr int VF = V.x * V.y * V.z;  // elements of one V field
+  static constexpr int OFF_V = 0;
+  static constexpr int OFF_BHP = OFF_V + V.padded();
+  static constexpr int OFF_BLP = OFF_BHP + BHP.padded();
+  static constexpr int OFF_BHQ = OFF_BLP + BLP.padded();
+  static constexpr int OFF_BLQ = OFF_BHQ + BHQ.padded();
+  static constexpr int OFF_RHO = OFF_BLQ + BLQ.padded();
+  static constexpr int OFF_WQ = OFF_RHO + RHO.padded();
+  static constexpr int OFF_WP = OFF_WQ + WQ.padded();
+  static constexpr int ELEMS = OFF_WP + WP.padded();
+  // elements the TMA delivers into a slot (the barrier's transaction count)
+  static constexpr int TX = V.elems() + BHP.elems() + BLP.elems() + BHQ.elems() + BLQ.elems() +
+                            RHO.elems() + WQ.elems() + WP.elems();
+};
+
+struct alignas(64) EmfMaps {
+  CUtensorMap v;       // first-sweep velocities V (2 of its 6 fields)
+  CUtensorMap bhp;     // B_h, component p, window along q
+  CUtensorMap blp[2];  // step-start B (per parity in FP64), component p
+  CUtensorMap bhq;     // B_h, component q, window along p
+  CUtensorMap blq[2];  // step-start B, component q
+  CUtensorMap rho;     // W_h density around the edges
+  CUtensorMap wq;      // weights of the q faces
+  CUtensorMap wp;      // weights of the p faces
+  int nt[3];
+};
+
+template <int D>
+__device__ __forceinline__ TileAt emf_at(const int nt[3], int t) {
+  const int a = t % nt[0], r = t / nt[0], b = r % nt[1], c = r / nt[1];
+  TileAt T;
+  T.x0 = NGH + 32 * a;
+  if constexpr (D == 2) {  // warps: faces along j, one plane k
+    T.y0 = NGH + 8 * b;
+    T.z0 = NGH + c;
+  } else {  // warps: faces along k, one row j
+    T.y0 = NGH + c;
+    T.z0 = NGH + 8 * b;
   }
-#pragma unroll
-  for (int a = 0; a < 3; a++) {
-    R v[8], lim[4];
-#pragma unroll
-    for (int t = 0; t < 8; t++) v[t] = msh[a * F::SB + t * TS];
-#pragma unroll
-    for (int u = 0; u < 4; u++) lim[u] = ms[a * F::LB + u * TS];
-    recon_lr<R>(v, lim, Wt, a1h, a2, mL[a], mR[a]);
-  }
-  flux_out<R, D, BG, false>(P, wk, lin(P, T.i, T.j, T.k), L, Rt, mL, mR, bn);
+  return T;
 }
 
-// Persistent flux sweep along D (entropy channel off).  Lane 0 of warp 0
-// also feeds the ring: it fills the first STAGES slots, and after each tile
-// waits until all 8 warps have released that tile's slot, then issues the
-// tile STAGES ahead into it; the other warps meanwhile compute the next
-// tile, whose copies were issued a tile earlier.
 template <typename R, int D, bool BG>
-__global__ void __launch_bounds__(kSweepThreads, SweepCfg<R>::CTAS)
-    k_flux_sweep(Params P, Work<R> wk, const __grid_constant__ FluxMaps maps) {
-  pdl_enter();
+struct EmfStage {
+  using E = EmfTile<D>;
+  using Maps = EmfMaps;
+  static constexpr int ELEMS = E::ELEMS;
+  static constexpr int TX = E::TX;
+  static constexpr int p = (D + 1) % 3, q = (D + 2) % 3;
+
+  __device__ static void issue(const Params& P, const Maps& m, int par, int t, R* s, uint64_t* bar) {
+    const TileAt T = emf_at<D>(m.nt, t);
+    const int x0 = T.x0, y0 = T.y0, z0 = T.z0;
+    if constexpr (D == 0) {  // i cells, j face y0, k faces z0..
+      tma_load_4d(s + E::OFF_V, &m.v, bar, x0, y0, z0 - 4, 0);
+      tma_load_4d(s + E::OFF_BHP, &m.bhp, bar, x0, y0, z0 - 4, 1);
+      tma_load_4d(s + E::OFF_BLP, &m.blp[par], bar, x0, y0, z0 - 2, 1);
+      tma_load_4d(s + E::OFF_BHQ, &m.bhq, bar, x0, y0 - 4, z0, 2);
+      tma_load_4d(s + E::OFF_BLQ, &m.blq[par], bar, x0, y0 - 2, z0, 2);
+      tma_load_4d(s + E::OFF_RHO, &m.rho, bar, x0, y0 - 1, z0 - 1, 0);
+      tma_load_4d(s + E::OFF_WQ, &m.wq, bar, 0, 2 * P.tmax + z0, 0, 0);
+      tma_load_4d(s + E::OFF_WP, &m.wp, bar, 0, P.tmax + y0, 0, 0);
+    } else if constexpr (D == 1) {  // i faces, j cell y0, k faces z0..
+      tma_load_4d(s + E::OFF_V, &m.v, bar, x0 - 4, y0, z0, 2);
+      tma_load_4d(s + E::OFF_BHP, &m.bhp, bar, x0 - 4, y0, z0, 2);
+      tma_load_4d(s + E::OFF_BLP, &m.blp[par], bar, x0 - 4, y0, z0, 2);
+      tma_load_4d(s + E::OFF_BHQ, &m.bhq, bar, x0, y0, z0 - 4, 0);
+      tma_load_4d(s + E::OFF_BLQ, &m.blq[par], bar, x0, y0, z0 - 2, 0);
+      tma_load_4d(s + E::OFF_RHO, &m.rho, bar, x0 - 4, y0, z0 - 1, 0);
+      tma_load_4d(s + E::OFF_WQ, &m.wq, bar, x0, T_WL0, 0, 0);
+      tma_load_4d(s + E::OFF_WP, &m.wp, bar, 0, 2 * P.tmax + z0, 0, 0);
+    } else {  // i faces, j faces y0.., k cell z0
+      tma_load_4d(s + E::OFF_V, &m.v, bar, x0, y0 - 4, z0, 4);
+      tma_load_4d(s + E::OFF_BHP, &m.bhp, bar, x0, y0 - 4, z0, 0);
+      tma_load_4d(s + E::OFF_BLP, &m.blp[par], bar, x0, y0 - 2, z0, 0);
+      tma_load_4d(s + E::OFF_BHQ, &m.bhq, bar, x0 - 4, y0, z0, 1);
+      tma_load_4d(s + E::OFF_BLQ, &m.blq[par], bar, x0 - 4, y0, z0, 1);
+      tma_load_4d(s + E::OFF_RHO, &m.rho, bar, x0 - 4, y0 - 1, z0, 0);
+      tma_load_4d(s + E::OFF_WQ, &m.wq, bar, 0, P.tmax + y0, 0, 0);
+      tma_load_4d(s + E::OFF_WP, &m.wp, bar, x0, T_WL0, 0, 0);
+    }
+  }
+
+  // one edge per thread
+  __device__ static void compute(const Params& P, const Work<R>& wk, const Maps& m, const R* s,
+                                 int t, int warp, int lane) {
+    const TileAt T = emf_at<D>(m.nt, t);
+    const int i = T.x0 + lane, j = T.y0 + (D == 2 ? warp : 0), k = T.z0 + (D == 2 ? 0 : warp);
+    if (!(i < NGH + P.n[0] + (D != 0) && j < NGH + P.n[1] + (D != 1) && k < NGH + P.n[2] + (D != 2)))
+      return;
+    const R a1h = (R)(0.5 * P.pdm_a1), a2 = (R)P.pdm_a2;
+    // stencil bases and tap strides of the windows along q and along p
+    const R *v0, *bp, *bpl, *bq, *bql;
+    constexpr int tq = D == 1 ? 1 : 32;  // slot stride of one tap along q
+    constexpr int tp = D == 2 ? 1 : 32;  // ... along p
+    R rho4;
+    const R* rh = s + E::OFF_RHO;
+    FaceWeights<R> Wq, Wp;
+    if constexpr (D == 0) {  // q = k rows of 32; p = j rows of 32 in the warp's k face
+      v0 = s + E::OFF_V + warp * 32 + lane;
+      bp = s + E::OFF_BHP + warp * 32 + lane;
+      bpl = s + E::OFF_BLP + warp * 32 + lane;
+      bq = s + E::OFF_BHQ + warp * 8 * 32 + lane;
+      bql = s + E::OFF_BLQ + warp * 4 * 32 + lane;
+      // (j-1,k-1) + (j-1,k) + (j,k-1) + (j,k); box rows [k][j]
+      const R* r = rh + lane;
+      rho4 = r[(warp * 2 + 0) * 32] + r[((warp + 1) * 2 + 0) * 32] + r[(warp * 2 + 1) * 32] +
+             r[((warp + 1) * 2 + 1) * 32];
+      load_fw_smem(s + E::OFF_WQ + warp * FW, Wq);
+      load_fw_smem(s + E::OFF_WP, Wp);
+    } else if constexpr (D == 1) {  // q = i in a row of 40; p = k rows of 32
+      v0 = s + E::OFF_V + warp * 40 + lane;
+      bp = s + E::OFF_BHP + warp * 40 + lane;
+      bpl = s + E::OFF_BLP + warp * 40 + lane + 2;
+      bq = s + E::OFF_BHQ + warp * 32 + lane;
+      bql = s + E::OFF_BLQ + warp * 32 + lane;
+      // (i-1,k-1) + (i-1,k) + (i,k-1) + (i,k); box rows of 40 along k
+      const R* r = rh + lane + 3;
+      rho4 = r[warp * 40] + r[(warp + 1) * 40] + r[warp * 40 + 1] + r[(warp + 1) * 40 + 1];
+      load_tap32(s + E::OFF_WQ + lane, Wq);
+      load_fw_smem(s + E::OFF_WP + warp * FW, Wp);
+    } else {  // q = j rows of 32; p = i in a row of 40
+      v0 = s + E::OFF_V + warp * 32 + lane;
+      bp = s + E::OFF_BHP + warp * 32 + lane;
+      bpl = s + E::OFF_BLP + warp * 32 + lane;
+      bq = s + E::OFF_BHQ + warp * 40 + lane;
+      bql = s + E::OFF_BLQ + warp * 40 + lane + 2;
+      // (i-1,j-1) + (i-1,j) + (i,j-1) + (i,j); box rows of 40 along j
+      const R* r = rh + lane + 3;
+      rho4 = r[warp * 40] + r[(warp + 1) * 40] + r[warp * 40 + 1] + r[(warp + 1) * 40 + 1];
+      load_fw_smem(s + E::OFF_WQ + warp * FW, Wq);
+      load_tap32(s + E::OFF_WP + lane, Wp);
+    }
+    R vav[2], bpL, bpR, bqL, bqR;
+#pragma unroll
+    for (int cc = 0; cc < 2; cc++) {  // second sweep along q, limited against itself
+      R v[8], lim[4], L, Rr;
+#pragma unroll
+      for (int u = 0; u < 8; u++) v[u] = v0[cc * E::VF + u * tq];
+#pragma unroll
+      for (int u = 0; u < 4; u++) lim[u] = v[u + 2];
+      recon_lr<R>(v, lim, Wq, a1h, a2, L, Rr);
+      vav[cc] = R(0.5) * (L + Rr);
+    }
+    {  // B_p along q
+      R v[8], lim[4];
+#pragma unroll
+      for (int u = 0; u < 8; u++) v[u] = bp[u * tq];
+#pragma unroll
+      for (int u = 0; u < 4; u++) lim[u] = bpl[u * tq];
+      recon_lr<R>(v, lim, Wq, a1h, a2, bpL, bpR);
+    }
+    {  // B_q along p
+      R v[8], lim[4];
+#pragma unroll
+      for (int u = 0; u < 8; u++) v[u] = bq[u * tp];
+#pragma unroll
+      for (int u = 0; u < 4; u++) lim[u] = bql[u * tp];
+      recon_lr<R>(v, lim, Wp, a1h, a2, bqL, bqR);
+    }
+    const long long x = lin(P, i, j, k);
+    const size_t fs = P.fs;
+    R b0p = R(0), b0q = R(0);
+    if constexpr (BG) {  // B0 averaged along the edge (B0Aedge*)
+      b0p = (R)P.bg[(size_t)(BG_EDGE + 3 * D + p) * fs + x];
+      b0q = (R)P.bg[(size_t)(BG_EDGE + 3 * D + q) * fs + x];
+    }
+    wk.E[x + (size_t)D * fs] =
+        emf_finish<R, BG>(P, vav[0], vav[1], bpL, bpR, bqL, bqR, b0p, b0q, rho4);
+  }
+};
+
+// ------------------------------------------------------------- pipeline
+
+template <class Stage, typename R>
+__host__ __device__ constexpr int slot_bytes() {
+  return Stage::ELEMS * (int)sizeof(R);
+}
+template <class Stage, typename R>
+__host__ __device__ constexpr int sweep_smem() {
+  return SweepCfg<R>::STAGES * slot_bytes<Stage, R>() + 2 * SweepCfg<R>::STAGES * 8 + 128;
+}
+
+// Persistent sweep: lane 0 of warp 0 also feeds the ring.  It fills the
+// first STAGES slots, and after each tile waits until all 8 warps have
+// released that tile's slot, then issues the tile STAGES ahead into it; the
+// other warps meanwhile compute the next tile, whose copies were issued a
+// tile earlier.  Every wait is bounded; a block that gives up records the
+// failure in S_FLAGS (2) and drains its copies in flight before it exits.
+template <class Stage, typename R>
+__device__ __forceinline__ void sweep_run(const Params& P, const Work<R>& wk,
+                                          const typename Stage::Maps& maps) {
   // stop flag, or an earlier pipeline wait that timed out: do nothing
   if (stopped(P) || P.scal[S_FLAGS] == 2.0) return;
-  using F = FluxTile<D>;
   constexpr int S = SweepCfg<R>::STAGES;
+  constexpr int SLOT = slot_bytes<Stage, R>();
+  constexpr int TXB = Stage::TX * (int)sizeof(R);  // bytes the copies of one tile deliver
+  static_assert(TXB <= SLOT, "slot holds its boxes");
   extern __shared__ unsigned char smem_dyn[];
   // TMA destinations on 128-byte boundaries (the launch adds 128 bytes)
-  unsigned char* smem_raw = reinterpret_cast<unsigned char*>(
+  unsigned char* base = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~static_cast<uintptr_t>(127));
-  R* slots = reinterpret_cast<R*>(smem_raw);
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + S * slot_bytes<R, D>());
+  R* slots = reinterpret_cast<R*>(base);
+  uint64_t* full = reinterpret_cast<uint64_t*>(base + S * SLOT);
   uint64_t* empty = full + S;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const bool feeder = threadIdx.x == 0;
   const int ntiles = maps.nt[0] * maps.nt[1] * maps.nt[2];
   const int par = sizeof(R) == 8 ? cur_buf(P) : 0;
-  const CUtensorMap* wl = &maps.wl[par];
-  const CUtensorMap* bnm = &maps.bn[par];
-  // issues the copies of the n-th tile of this block (tile index t) into its slot
   auto issue = [&](int n, int t) {
     const int q = n % S;
-    const TileAt<D> T = tile_at<D>(maps.nt, t, 0, 0);
-    R* s = slots + (size_t)q * F::ELEMS;
-    mbar_arrive_expect_tx(&full[q], slot_bytes<R, D>());
-    tma_load_4d(s + F::OFF_WH, &maps.wh, &full[q], T.sx, T.sy, T.sz, 0);
-    tma_load_4d(s + F::OFF_WL, wl, &full[q], T.sx, T.ly, T.lz, 0);
-    tma_load_4d(s + F::OFF_MSH, &maps.msh, &full[q], T.sx, T.sy, T.sz, 0);
-    tma_load_4d(s + F::OFF_MS, &maps.ms, &full[q], T.sx, T.ly, T.lz, 0);
-    // weights: D = 0 rows T_WL0.. of the faces f0..f0+31 of axis 0; else the
-    // records of faces f0..f0+7 of axis D
-    const int f0 = D == 0 ? T.sx + NGH : (D == 1 ? T.sy + NGH : T.sz + NGH);
-    if constexpr (D == 0) tma_load_4d(s + F::OFF_W, &maps.wt, &full[q], f0, T_WL0, 0, 0);
-    else tma_load_4d(s + F::OFF_W, &maps.wt, &full[q], 0, D * P.tmax + f0, 0, 0);
-    // B_n at the tile's faces
-    if constexpr (D == 0) tma_load_4d(s + F::OFF_BN, bnm, &full[q], f0, T.sy, T.sz, 0);
-    else if constexpr (D == 1) tma_load_4d(s + F::OFF_BN, bnm, &full[q], T.sx, f0, T.sz, 1);
-    else tma_load_4d(s + F::OFF_BN, bnm, &full[q], T.sx, T.sy, f0, 2);
+    mbar_arrive_expect_tx(&full[q], TXB);
+    Stage::issue(P, maps, par, t, slots + (size_t)q * Stage::ELEMS, &full[q]);
   };
   int issued = 0;  // feeder only: tiles whose copies were issued
   if (feeder) {
     for (int q = 0; q < S; q++) {
       mbar_init(&full[q], 1);
-      mbar_init(&empty[q], kConsumerWarps);
+      mbar_init(&empty[q], kWarps);
     }
     fence_mbar_init();
     for (int t = blockIdx.x; t < ntiles && issued < S; t += gridDim.x) issue(issued++, t);
@@ -317,8 +484,7 @@ __global__ void __launch_bounds__(kSweepThreads, SweepCfg<R>::CTAS)
       ok = false;
       break;
     }
-    const TileAt<D> T = tile_at<D>(maps.nt, t, warp, lane);
-    flux_tile<R, D, BG>(P, wk, slots + (size_t)q * F::ELEMS, T, warp, lane);
+    Stage::compute(P, wk, maps, slots + (size_t)q * Stage::ELEMS, t, warp, lane);
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[q]);
     if (feeder) {
@@ -335,11 +501,35 @@ __global__ void __launch_bounds__(kSweepThreads, SweepCfg<R>::CTAS)
   }
   if (feeder) {
     // the copies of the tiles issued last must land before the block exits
-    for (int m = issued > S ? issued - S : 0; m < issued; m++)
-      if (!mbar_wait(&full[m % S], (m / S) & 1)) ok = false;
+    for (int k = issued > S ? issued - S : 0; k < issued; k++)
+      if (!mbar_wait(&full[k % S], (k / S) & 1)) ok = false;
   }
   if (!ok) P.scal[S_FLAGS] = 2.0;
 }
+
+template <typename R, int D, bool BG>
+__global__ void __launch_bounds__(kSweepThreads, SweepCfg<R>::CTAS)
+    k_flux_sweep(Params P, Work<R> wk, const __grid_constant__ FluxMaps maps) {
+  pdl_enter();
+  sweep_run<FluxStage<R, D, BG>, R>(P, wk, maps);
+}
+
+template <typename R, int D, bool BG>
+__global__ void __launch_bounds__(kSweepThreads, SweepCfg<R>::CTAS)
+    k_emf_sweep(Params P, Work<R> wk, const __grid_constant__ EmfMaps maps) {
+  pdl_enter();
+  sweep_run<EmfStage<R, D, BG>, R>(P, wk, maps);
+}
+
+template <typename R, int D>
+constexpr bool smem_fits() {
+  return (size_t)sweep_smem<FluxStage<R, D, false>, R>() * SweepCfg<R>::CTAS <= 228 * 1024 &&
+         (size_t)sweep_smem<EmfStage<R, D, false>, R>() * SweepCfg<R>::CTAS <= 228 * 1024;
+}
+static_assert(smem_fits<double, 0>() && smem_fits<double, 1>() && smem_fits<double, 2>(),
+              "FP64 sweep blocks per SM");
+static_assert(smem_fits<float, 0>() && smem_fits<float, 1>() && smem_fits<float, 2>(),
+              "FP32 sweep blocks per SM");
 
 // ------------------------------------------------------------------ host
 
@@ -361,77 +551,77 @@ static EncodeTiledFn encode_fn() {
   return fn;
 }
 
-// a 4-D map (i, j, k, field) over nf fields of one array in the state's
-// layout, read in boxes of bx x by x bz x bf elements
+// a 4-D map over a dense array of dims d[0..3] (elements, d[0] fastest;
+// strides in bytes), read in boxes b
 template <typename R>
-static bool make_map(CUtensorMap* m, const R* base, int nf, const Params& P, int bx, int by, int bz,
-                     int bf) {
+static bool encode(CUtensorMap* m, const R* base, const cuuint64_t d[4], const cuuint64_t st[3],
+                   const Box& b) {
   EncodeTiledFn fn = encode_fn();
   if (!fn || !base) return false;
-  const cuuint64_t es = sizeof(R);
-  const cuuint64_t dims[4] = {(cuuint64_t)P.N[0], (cuuint64_t)P.N[1], (cuuint64_t)P.N[2], (cuuint64_t)nf};
-  const cuuint64_t strides[3] = {(cuuint64_t)P.pitch * es, (cuuint64_t)P.sk * es, (cuuint64_t)P.fs * es};
-  const cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz, (cuuint32_t)bf};
+  const cuuint32_t bx[4] = {(cuuint32_t)b.x, (cuuint32_t)b.y, (cuuint32_t)b.z, (cuuint32_t)b.f};
   const cuuint32_t el[4] = {1, 1, 1, 1};
   const CUresult r =
       fn(m, sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
-         const_cast<R*>(base), dims, strides, box, el, CU_TENSOR_MAP_INTERLEAVE_NONE,
-         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+         const_cast<R*>(base), d, st, bx, el, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
 
-// a 4-D map over a plain array of dims d[0..3] (elements, d[0] fastest)
+// nf fields of one array in the state's layout (i, j, k, field)
 template <typename R>
-static bool make_map_dims(CUtensorMap* m, const R* base, const cuuint64_t d[4], const int box[4]) {
-  EncodeTiledFn fn = encode_fn();
-  if (!fn || !base) return false;
+static bool field_map(CUtensorMap* m, const R* base, int nf, const Params& P, const Box& b) {
   const cuuint64_t es = sizeof(R);
-  const cuuint64_t strides[3] = {d[0] * es, d[0] * d[1] * es, d[0] * d[1] * d[2] * es};
-  const cuuint32_t bx[4] = {(cuuint32_t)box[0], (cuuint32_t)box[1], (cuuint32_t)box[2], (cuuint32_t)box[3]};
-  const cuuint32_t el[4] = {1, 1, 1, 1};
-  const CUresult r =
-      fn(m, sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
-         const_cast<R*>(base), d, strides, bx, el, CU_TENSOR_MAP_INTERLEAVE_NONE,
-         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  return r == CUDA_SUCCESS;
+  const cuuint64_t d[4] = {(cuuint64_t)P.N[0], (cuuint64_t)P.N[1], (cuuint64_t)P.N[2], (cuuint64_t)nf};
+  const cuuint64_t st[3] = {(cuuint64_t)P.pitch * es, (cuuint64_t)P.sk * es, (cuuint64_t)P.fs * es};
+  return encode<R>(m, base, d, st, b);
+}
+
+// PDM weights: the per-axis tables [axis][NTAB][tmax] for tap-major boxes,
+// the packed face records [axis * tmax + f][FW] otherwise
+template <typename R>
+static bool weight_map(CUtensorMap* m, const Work<R>& w, const Params& P, const Box& b) {
+  const cuuint64_t es = sizeof(R), tm = (cuuint64_t)P.tmax;
+  if (b.x == kTap32.x && b.y == kTap32.y) {
+    const cuuint64_t d[4] = {tm, (cuuint64_t)NTAB, 3, 1};
+    const cuuint64_t st[3] = {tm * es, tm * NTAB * es, tm * NTAB * 3 * es};
+    return encode<R>(m, w.tab, d, st, b);
+  }
+  const cuuint64_t d[4] = {(cuuint64_t)FW, 3 * tm, 1, 1};
+  const cuuint64_t st[3] = {FW * es, FW * 3 * tm * es, FW * 3 * tm * es};
+  return encode<R>(m, w.fw, d, st, b);
+}
+
+// the limiters' step-start references: FP64 the state buffer of parity b,
+// FP32 its copy (the same for both parities)
+template <typename R>
+static const R* lim_state(const Params& P, const Work<R>& w, int b) {
+  return sizeof(R) == 8 ? reinterpret_cast<const R*>(P.Wbuf[b]) : w.Wl;
+}
+template <typename R>
+static const R* lim_face(const Params& P, const Work<R>& w, int b) {
+  return sizeof(R) == 8 ? reinterpret_cast<const R*>(P.Bbuf[b]) : w.Bl;
 }
 
 template <typename R, int D>
 static bool make_flux_maps(FluxMaps& m, const Params& P, const Work<R>& w) {
   using F = FluxTile<D>;
-  bool ok = make_map<R>(&m.wh, w.Wh, 6, P, F::SX, F::SY, F::SZ, F::NG) &&
-            make_map<R>(&m.msh, w.Msh, 3, P, F::SX, F::SY, F::SZ, 3) &&
-            make_map<R>(&m.ms, w.Ms, 3, P, F::LX, F::LY, F::LZ, 3);
-  // face field normal to the faces: box (32, 8, 1), (32, 8, 1) or (32, 1, 8)
-  const int bx = 32, by = D == 2 ? 1 : 8, bz = D == 2 ? 8 : 1;
-  for (int b = 0; b < 2 && ok; b++) {
-    const R* lim = sizeof(R) == 8 ? reinterpret_cast<const R*>(P.Wbuf[b]) : w.Wl;
-    const R* fb = sizeof(R) == 8 ? reinterpret_cast<const R*>(P.Bbuf[b]) : w.Bl;
-    ok = make_map<R>(&m.wl[b], lim, 6, P, F::LX, F::LY, F::LZ, F::NG) &&
-         make_map<R>(&m.bn[b], fb, 3, P, bx, by, bz, 1);
-  }
-  if (ok) {
-    const cuuint64_t tm = (cuuint64_t)P.tmax;
-    if (D == 0) {  // the per-axis tables [axis][NTAB][tmax]
-      const cuuint64_t d[4] = {tm, (cuuint64_t)NTAB, 3, 1};
-      const int box[4] = {32, 18, 1, 1};
-      ok = make_map_dims<R>(&m.wt, w.tab, d, box);
-    } else {       // the packed face records [axis * tmax + f][FW]
-      const cuuint64_t d[4] = {(cuuint64_t)FW, 3 * tm, 1, 1};
-      const int box[4] = {FW, 8, 1, 1};
-      ok = make_map_dims<R>(&m.wt, w.fw, d, box);
-    }
-  }
+  const Box S5{F::S.x, F::S.y, F::S.z, F::NG}, L5{F::L.x, F::L.y, F::L.z, F::NG};
+  const Box S3{F::S.x, F::S.y, F::S.z, 3}, L3{F::L.x, F::L.y, F::L.z, 3};
+  bool ok = field_map<R>(&m.wh, w.Wh, 6, P, S5) && field_map<R>(&m.msh, w.Msh, 3, P, S3) &&
+            field_map<R>(&m.ms, w.Ms, 3, P, L3) && weight_map<R>(&m.wt, w, P, F::WT);
+  for (int b = 0; b < 2 && ok; b++)
+    ok = field_map<R>(&m.wl[b], lim_state<R>(P, w, b), 6, P, L5) &&
+         field_map<R>(&m.bn[b], lim_face<R>(P, w, b), 3, P, F::BN);
   const int n0 = P.n[0], n1 = P.n[1], n2 = P.n[2];
-  if (D == 0) {
+  if (D == 0) {  // i-face tiles, j-row tiles, k planes
     m.nt[0] = (n0 + 1 + 31) / 32;
     m.nt[1] = (n1 + 7) / 8;
     m.nt[2] = n2;
-  } else if (D == 1) {
+  } else if (D == 1) {  // i tiles, j-face tiles, k planes
     m.nt[0] = (n0 + 31) / 32;
     m.nt[1] = (n1 + 1 + 7) / 8;
     m.nt[2] = n2;
-  } else {
+  } else {  // i tiles, k-face tiles, j rows
     m.nt[0] = (n0 + 31) / 32;
     m.nt[1] = (n2 + 1 + 7) / 8;
     m.nt[2] = n1;
@@ -439,10 +629,46 @@ static bool make_flux_maps(FluxMaps& m, const Params& P, const Work<R>& w) {
   return ok;
 }
 
+template <typename R, int D>
+static bool make_emf_maps(EmfMaps& m, const Params& P, const Work<R>& w) {
+  using E = EmfTile<D>;
+  bool ok = field_map<R>(&m.v, w.V, 6, P, E::V) && field_map<R>(&m.bhp, w.Bh, 3, P, E::BHP) &&
+            field_map<R>(&m.bhq, w.Bh, 3, P, E::BHQ) && field_map<R>(&m.rho, w.Wh, 6, P, E::RHO) &&
+            weight_map<R>(&m.wq, w, P, E::WQ) && weight_map<R>(&m.wp, w, P, E::WP);
+  for (int b = 0; b < 2 && ok; b++)
+    ok = field_map<R>(&m.blp[b], lim_face<R>(P, w, b), 3, P, E::BLP) &&
+         field_map<R>(&m.blq[b], lim_face<R>(P, w, b), 3, P, E::BLQ);
+  const int n0 = P.n[0], n1 = P.n[1], n2 = P.n[2];
+  if (D == 0) {  // i-cell tiles, k-face tiles, j faces
+    m.nt[0] = (n0 + 31) / 32;
+    m.nt[1] = (n2 + 1 + 7) / 8;
+    m.nt[2] = n1 + 1;
+  } else if (D == 1) {  // i-face tiles, k-face tiles, j cells
+    m.nt[0] = (n0 + 1 + 31) / 32;
+    m.nt[1] = (n2 + 1 + 7) / 8;
+    m.nt[2] = n1;
+  } else {  // i-face tiles, j-face tiles, k cells
+    m.nt[0] = (n0 + 1 + 31) / 32;
+    m.nt[1] = (n1 + 1 + 7) / 8;
+    m.nt[2] = n2;
+  }
+  return ok;
+}
+
+struct SweepSet {
+  FluxMaps flux[3];
+  EmfMaps emf[3];
+  int sms = 0;
+};
+
 template <typename R, int D, bool BG>
 static cudaError_t allow_smem() {
-  return cudaFuncSetAttribute(k_flux_sweep<R, D, BG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              sweep_smem<R, D>());
+  cudaError_t e = cudaFuncSetAttribute(k_flux_sweep<R, D, BG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       sweep_smem<FluxStage<R, D, BG>, R>());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_emf_sweep<R, D, BG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             sweep_smem<EmfStage<R, D, BG>, R>());
+  return e;
 }
 
 template <typename R>
@@ -453,7 +679,8 @@ SweepSet* sweep_create(const Params& P, const Work<R>& w) {
   bool ok = cudaGetDevice(&dev) == cudaSuccess &&
             cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess;
   ok = ok && make_flux_maps<R, 0>(s->flux[0], P, w) && make_flux_maps<R, 1>(s->flux[1], P, w) &&
-       make_flux_maps<R, 2>(s->flux[2], P, w);
+       make_flux_maps<R, 2>(s->flux[2], P, w) && make_emf_maps<R, 0>(s->emf[0], P, w) &&
+       make_emf_maps<R, 1>(s->emf[1], P, w) && make_emf_maps<R, 2>(s->emf[2], P, w);
   ok = ok && allow_smem<R, 0, false>() == cudaSuccess && allow_smem<R, 1, false>() == cudaSuccess &&
        allow_smem<R, 2, false>() == cudaSuccess && allow_smem<R, 0, true>() == cudaSuccess &&
        allow_smem<R, 1, true>() == cudaSuccess && allow_smem<R, 2, true>() == cudaSuccess;
@@ -469,9 +696,9 @@ template SweepSet* sweep_create<float>(const Params&, const Work<float>&);
 
 void sweep_destroy(SweepSet* s) { delete s; }
 
-template <typename R, int D, bool BG>
-static void launch_sweep_d(const SweepSet* sw, const Params& P, const Work<R>& w, cudaStream_t st) {
-  const FluxMaps& m = sw->flux[D];
+template <class Stage, typename R, class Maps, class K>
+static void launch_persistent(K kern, const SweepSet* sw, const Params& P, const Work<R>& w,
+                              const Maps& m, cudaStream_t st) {
   const int ntiles = m.nt[0] * m.nt[1] * m.nt[2];
   const int grid = std::max(1, std::min(ntiles, sw->sms * SweepCfg<R>::CTAS));
   cudaLaunchAttribute at[1];
@@ -480,12 +707,21 @@ static void launch_sweep_d(const SweepSet* sw, const Params& P, const Work<R>& w
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(kSweepThreads);
-  cfg.dynamicSmemBytes = sweep_smem<R, D>();
+  cfg.dynamicSmemBytes = sweep_smem<Stage, R>();
   cfg.stream = st;
   cfg.attrs = at;
   cfg.numAttrs = GOP_SWEEP_PDL ? 1 : 0;
-  cudaLaunchKernelEx(&cfg, k_flux_sweep<R, D, BG>, P, w, m);
+  cudaLaunchKernelEx(&cfg, kern, P, w, m);
   count_launches(1);
+}
+
+template <typename R, int D, bool BG>
+static void launch_flux_d(const SweepSet* sw, const Params& P, const Work<R>& w, cudaStream_t st) {
+  launch_persistent<FluxStage<R, D, BG>, R>(k_flux_sweep<R, D, BG>, sw, P, w, sw->flux[D], st);
+}
+template <typename R, int D, bool BG>
+static void launch_emf_d(const SweepSet* sw, const Params& P, const Work<R>& w, cudaStream_t st) {
+  launch_persistent<EmfStage<R, D, BG>, R>(k_emf_sweep<R, D, BG>, sw, P, w, sw->emf[D], st);
 }
 
 template <typename R>
@@ -494,9 +730,9 @@ bool launch_flux_sweep(const SweepSet* sw, const Params& P, const Work<R>& w, in
   if (!sw || P.ps_live) return false;  // the entropy channel runs the per-face kernels
   const bool bg = P.bg != nullptr;
   switch (D) {
-    case 0: bg ? launch_sweep_d<R, 0, true>(sw, P, w, st) : launch_sweep_d<R, 0, false>(sw, P, w, st); break;
-    case 1: bg ? launch_sweep_d<R, 1, true>(sw, P, w, st) : launch_sweep_d<R, 1, false>(sw, P, w, st); break;
-    default: bg ? launch_sweep_d<R, 2, true>(sw, P, w, st) : launch_sweep_d<R, 2, false>(sw, P, w, st); break;
+    case 0: bg ? launch_flux_d<R, 0, true>(sw, P, w, st) : launch_flux_d<R, 0, false>(sw, P, w, st); break;
+    case 1: bg ? launch_flux_d<R, 1, true>(sw, P, w, st) : launch_flux_d<R, 1, false>(sw, P, w, st); break;
+    default: bg ? launch_flux_d<R, 2, true>(sw, P, w, st) : launch_flux_d<R, 2, false>(sw, P, w, st); break;
   }
   return true;
 }
@@ -504,5 +740,21 @@ template bool launch_flux_sweep<double>(const SweepSet*, const Params&, const Wo
                                         cudaStream_t);
 template bool launch_flux_sweep<float>(const SweepSet*, const Params&, const Work<float>&, int,
                                        cudaStream_t);
+
+template <typename R>
+bool launch_emf_sweep(const SweepSet* sw, const Params& P, const Work<R>& w, int D, cudaStream_t st) {
+  if (!sw) return false;
+  const bool bg = P.bg != nullptr;
+  switch (D) {
+    case 0: bg ? launch_emf_d<R, 0, true>(sw, P, w, st) : launch_emf_d<R, 0, false>(sw, P, w, st); break;
+    case 1: bg ? launch_emf_d<R, 1, true>(sw, P, w, st) : launch_emf_d<R, 1, false>(sw, P, w, st); break;
+    default: bg ? launch_emf_d<R, 2, true>(sw, P, w, st) : launch_emf_d<R, 2, false>(sw, P, w, st); break;
+  }
+  return true;
+}
+template bool launch_emf_sweep<double>(const SweepSet*, const Params&, const Work<double>&, int,
+                                       cudaStream_t);
+template bool launch_emf_sweep<float>(const SweepSet*, const Params&, const Work<float>&, int,
+                                      cudaStream_t);
 
 }  // namespace gop

@@ -153,14 +153,14 @@ int gop_get_stats(gop_instance *h, gop_stats *out);
  * following steps.  reps: timed launches per candidate (0 = 3); chosen
  * (optional, 11 ints) receives the picked candidate index per launch. */
 #define GOP_NTUNE 11
-#define GOP_TUNE_SWEEP 14 /* chosen[] value of a flux launch: the tile-staged sweep kernel */
+#define GOP_TUNE_SWEEP 14 /* chosen[] value of a flux or EMF launch: the tile-staged sweep kernel */
 int gop_autotune(gop_instance *h, int reps, int *chosen);
 
-/* Kernel choice for the face flux of each axis: on (the default) runs the
- * tile-staged sweep kernels (shared-memory tiles filled by the Tensor Memory
- * Accelerator, one persistent block per SM slot) wherever they apply, off
- * the per-face kernels; both give the same results.  With the entropy
- * channel live the per-face kernels always run.  GOP_ENODEV if the sweep
+/* Kernel choice for the face fluxes and edge EMFs: on (the default) runs
+ * the tile-staged sweep kernels (shared-memory tiles filled by the Tensor
+ * Memory Accelerator, persistent blocks) wherever they apply, off the
+ * per-point kernels; both give the same results.  With the entropy channel
+ * live the per-face flux kernels always run.  GOP_ENODEV if the sweep
  * kernels could not be set up for this instance. */
 int gop_set_sweep(gop_instance *h, int on);
 
