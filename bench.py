@@ -124,18 +124,81 @@ class ClockSampler:
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_baseline(n=(64, 64, 64), steps=12):
-    """GAMERA-OP's own solver on this host's cores (bounded sample)."""
+def host_cores():
+    """Physical cores of this host (logical CPUs when it cannot tell)."""
+    try:
+        seen = set()
+        phys = core = None
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("physical id"):
+                phys = line.split(":")[1].strip()
+            elif line.startswith("core id"):
+                core = line.split(":")[1].strip()
+                seen.add((phys, core))
+        if seen:
+            return len(seen)
+    except OSError:
+        pass
+    return os.cpu_count() or 1
+
+
+def rank_dims(cores, n):
+    """The reference's process grid for about `cores` ranks: the largest
+    power of two not above it, split over the axes as evenly as the grid
+    divides (GAMERA-OP needs every axis divisible by its process count)."""
+    r = 1
+    while r * 2 <= max(1, cores):
+        r *= 2
+    dims = [1, 1, 1]
+    a = 0
+    while r > 1:
+        for _ in range(3):
+            if n[a] % (dims[a] * 2) == 0 and n[a] // (dims[a] * 2) >= 8:
+                dims[a] *= 2
+                r //= 2
+                a = (a + 1) % 3
+                break
+            a = (a + 1) % 3
+        else:
+            break
+    return tuple(dims)
+
+
+def ref_bytes(n, dims):
+    """Host memory of a reference run: about 268 doubles per ghost-extended
+    point of every rank's block (its state, work and geometry arrays)."""
+    pts = 1
+    for a in range(3):
+        pts *= n[a] // dims[a] + 9
+    return 268 * 8 * pts * dims[0] * dims[1] * dims[2]
+
+
+def mem_available():
+    try:
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable:"):
+                return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return 0
+
+
+def cpu_baseline(n=(128, 128, 128), steps=4):
+    """GAMERA-OP's own solver on this host's cores in its README mode (one
+    process of one thread per core), a bounded sample of the blast."""
     try:
         import ref_run
         if ref_run.available("cart", "release"):
-            thr = os.cpu_count() or 1
-            r = ref_run.run(n, steps, problem="blast", flavor="release", keep_output=False,
-                            threads=thr, timeout=600)
+            dims = rank_dims(host_cores(), n)
+            ranks = dims[0] * dims[1] * dims[2]
+            r = ref_run.run(n, steps + 1, problem="blast", flavor="release", keep_output=False,
+                            threads=1, dims=dims, timeout=900,
+                            env={"GOP_BC": "pppppp", "GOP_DOMAIN": "-0.5,0.5,-0.5,0.5,-0.5,0.5"})
             cells = n[0] * n[1] * n[2]
             v = cells * r.wall_steps / r.wall_seconds / 1e6
-            return {"value": round(v, 4), "unit": UNIT, "cores": thr, "kind": "reference",
-                    "sample": f"reference Release build (OpenMP, {thr} threads), blast {n[0]}^3, "
+            return {"value": round(v, 4), "unit": UNIT, "cores": ranks, "kind": "reference",
+                    "sample": f"reference Release build, {ranks} ranks x 1 thread "
+                              f"(process grid {dims[0]}x{dims[1]}x{dims[2]}), blast {n[0]}^3, "
                               f"{r.wall_steps} timed steps after 1"}
     except Exception:  # reference binary missing or failed: time the oracle port
         pass
@@ -155,39 +218,58 @@ def cpu_baseline(n=(64, 64, 64), steps=12):
 
 
 def run_reference(args, rank):
+    """GAMERA-OP's own CPU solver (Release build) on this host's cores in its
+    README mode, mpirun -n N with one thread per rank, through the fork-based
+    MPI stand-in: N = the host's physical cores (rounded down to a power of
+    two that divides the grid), on the workload's own grid when the host has
+    the memory for it."""
     if rank != 0:
         return
     import ref_run
-    n = (64, 64, 64)
     line = {"impl": "reference", "metric": METRIC, "unit": UNIT, "higher_is_better": True,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup}
     if not ref_run.available("cart", "release"):
         line["unavailable"] = "reference binary oracle/_ref/ref_cart_release_* is not built"
         print(json.dumps(line))
         return
-    thr = os.cpu_count() or 1
+    full = (args.n,) * 3
+    cores = host_cores()
+    n, why = full, None
+    need, avail = ref_bytes(full, rank_dims(cores, full)), mem_available()
+    if avail and need > 0.8 * avail:
+        n = (128, 128, 128)
+        why = (f"host RAM: {args.n}^3 needs about {need / 2**30:.0f} GiB, "
+               f"{avail / 2**30:.0f} GiB available")
+    dims = rank_dims(cores, n)
+    ranks = dims[0] * dims[1] * dims[2]
     r = ref_run.run(n, args.warmup + args.steps + 1, problem="blast", flavor="release",
-                    keep_output=False, threads=thr, env={"GOP_SHIM_TIMING": "2"}, timeout=3000)
+                    keep_output=False, threads=1, dims=dims,
+                    env={"GOP_SHIM_TIMING": "2", "GOP_BC": "pppppp",
+                         "GOP_DOMAIN": "-0.5,0.5,-0.5,0.5,-0.5,0.5"}, timeout=3000)
     starts = r.step_starts
     w = args.warmup
     t = starts[w + args.steps] - starts[w]
     cells = n[0] * n[1] * n[2]
     v = cells * args.steps / t / 1e6
     durs = np.diff(starts[w:w + args.steps + 1]) * 1e3
+    cfg = {"workload": f"blast3d_periodic_{args.n}^3_{args.precision}",
+           "grid": list(full),
+           "problem": "blast p_in=10 p_out=0.1 r=0.1 B=(1/sqrt2,1/sqrt2,0) gamma=5/3 CFL=0.3",
+           "ranks": ranks, "process_grid": list(dims), "threads_per_rank": 1,
+           "mode": "mpirun -n N, OMP_NUM_THREADS=1 (the reference README's mode), "
+                   "through the fork-based MPI stand-in"}
+    if n != full:
+        cfg["sample_grid"] = list(n)
+        cfg["note"] = f"each step timed at {n[0]}^3 instead of {args.n}^3: {why}"
     line.update({
         "value": round(v, 4), "ms_per_step": round(t / args.steps * 1e3, 3),
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"blast3d_periodic_{args.n}^3_{args.precision}",
-                   "grid": [args.n] * 3,
-                   "problem": "blast p_in=10 p_out=0.1 r=0.1 B=(1/sqrt2,1/sqrt2,0) gamma=5/3 CFL=0.3",
-                   "sample_grid": list(n),
-                   "note": f"bounded sample: each step of the {args.n}^3 workload timed on the "
-                           f"same problem at 64^3 (the reference computes in FP64)"},
+        "config": cfg,
         "latency_ms": {"p50": round(float(np.percentile(durs, 50)), 3),
                        "p99": round(float(np.percentile(durs, 99)), 3)},
-        "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": thr, "kind": "reference",
-                         "sample": f"blast 64^3, {args.steps} steps after {w} warm-up, "
-                                   f"OpenMP {thr} threads, Release flags"},
+        "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": ranks, "kind": "reference",
+                         "sample": f"blast {n[0]}^3, {args.steps} steps after {w} warm-up, "
+                                   f"{ranks} ranks x 1 thread, Release flags"},
         "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     })
     print(json.dumps(line))
@@ -204,6 +286,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="default workload: skip the mixed-precision run beside the FP64 one")
+    ap.add_argument("--no-batched-sample", action="store_true",
+                    help="default workload: skip the bounded batched sample")
     ap.add_argument("--workload", default="blast256",
                     choices=["blast256", "batched", "served", "ot", "sphere"],
                     help="blast256: the single 256^3 grid (default); batched: 96 uneven "
@@ -308,6 +394,14 @@ def main():
     e2e = None
     if not args.no_e2e:
         e2e = measure_e2e(gop, torch, n, prec, args, max_all, barrier, world)
+    # the metric's own comparison: the mixed path on the same grid and steps,
+    # its rate against this plain FP64 rate and its error against this run
+    mixed = None
+    if prec == gop.PREC_FP64 and not args.no_mixed:
+        mixed = measure_mixed(gop, torch, n, args, inst, value, max_all, barrier, world)
+    batched = None
+    if prec == gop.PREC_FP64 and not args.no_batched_sample:
+        batched = batched_sample(args, gop, torch, dist, rank, world, local, max_all, barrier)
 
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
@@ -338,6 +432,10 @@ def main():
         line["clocks"] = clk
     if e2e:
         line["e2e"] = e2e
+    if mixed:
+        line["mixed"] = mixed
+    if batched:
+        line["batched_sample"] = batched
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     if rank == 0:
@@ -345,6 +443,66 @@ def main():
     inst.close()
     if dist is not None:
         dist.destroy_process_group()
+
+
+def measure_mixed(gop, torch, n, args, plain, plain_value, max_all, barrier, world):
+    """The mixed path (FP32 reconstruction, fluxes and EMFs; FP64 state,
+    AB2, update and pressure recovery) on the same blast grid: K steps timed
+    after W warm-up steps like the plain run, then stepped on to the plain
+    instance's step count and compared with it variable by variable."""
+    from gop import accuracy
+    mx = gop.make(gop.PROBLEM_BLAST, n, precision=gop.PREC_MIXED)
+    stream = torch.cuda.Stream()
+    mx.set_stream(stream.cuda_stream)
+    mx.prepare()
+    if not args.no_autotune:
+        mx.autotune(reps=2)
+    with torch.cuda.stream(stream):
+        mx.step(args.warmup)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize()
+        a.record(stream)
+        mx.step(args.steps, sync=False)
+        b.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    ms = max_all(a.elapsed_time(b))
+    cells = n[0] * n[1] * n[2]
+    value = world * cells * args.steps / (ms / 1e3) / 1e6
+    steps_plain = plain.stats()["steps"]
+    extra = steps_plain - mx.stats()["steps"]
+    if extra > 0:
+        mx.step(extra)
+    which = ("gas", "face_b")
+    errs = accuracy.rel_l1(n, mx.download(which), plain.download(which))
+    worst, var = accuracy.worst(errs)
+    st = mx.stats()
+    mx.close()
+    return {"value": round(value, 3), "unit": UNIT, "ms_per_step": round(ms / args.steps, 4),
+            "ratio_vs_plain_fp64": round(value / plain_value, 3),
+            "dtype": "f32 reconstruction/flux/EMF, f64 state/AB2/update/p recovery",
+            "accuracy_vs_fp64": {"max_rel_l1": worst, "variable": var,
+                                 "rel_l1": {k: float(f"{v:.3e}") for k, v in errs.items()},
+                                 "steps": int(st["steps"]), "tolerance": 1e-5},
+            "divb_max": st["divb_max"]}
+
+
+def batched_sample(args, gop, torch, dist, rank, world, local, max_all, barrier):
+    """A bounded sample of the batched workload inside the default run: the
+    first 16 grids of the seeded 96-grid draw, 100 steps each, in one batch
+    (mixed) against the same grids one at a time on the plain FP64 path."""
+    import copy
+    a = copy.copy(args)
+    a.members, a.steps = 16, 100
+    line = bench_batched(a, gop, torch, dist, rank, world, local, max_all, barrier)
+    keep = ("value", "unit", "ms_per_step", "plain_fp64_one_at_a_time", "mixed_one_at_a_time",
+            "speedup_vs_plain_fp64", "accuracy_vs_fp64")
+    out = {k: line[k] for k in keep if k in line}
+    out["config"] = {k: line["config"][k] for k in ("workload", "members", "grids", "cells",
+                                                   "steps_per_member", "seed")}
+    out["config"]["sample"] = "first 16 grids of the seeded draw of 96, 100 steps each"
+    return out
 
 
 def _accuracy(gop, n, got, want):

@@ -2,13 +2,13 @@
 // without allocating any memory.
 //
 // Who needs this: a host that already keeps its grid in device memory and
-// has to ask "what dt does this state allow?" from a place where allocating
-// is off limits -- between the capture calls of a CUDA graph (cudaMalloc is
-// not capturable and would break the capture), inside a serving loop whose
-// device memory was reserved once at start-up and may not grow, or from a
-// host program that hands the library only the pointers it owns.  The
-// instance API (gop_create / gop_prepare) needs its own buffers; this entry
-// point needs none.
+// has to ask "what dt does this state allow?" where it may not allocate --
+// a serving loop whose device memory was reserved once at start-up and may
+// not grow (an allocation there can fail, or wait for the whole device,
+// since cudaMalloc and cudaFree synchronise with running work), or a host
+// program that owns all of its device buffers and hands the library only
+// pointers.  The instance API (gop_create / gop_prepare) needs its own
+// buffers; this entry point needs none.
 //
 // Its only scratch is g_cfl_scratch below: a file-scope device array of
 // GOP_NOALLOC_SCRATCH_DOUBLES doubles (64 KiB) that every GPU loading this
@@ -46,6 +46,8 @@ struct Args {
   double gamma, cfl, ca, ca2;
   const double* gas;  // [6][NI][NJ][NK], k fastest (reference layout)
   const double* fb;   // [3][NI][NJ][NK]
+  const double* b0;   // background field at the cell centroid [3][NI][NJ][NK], or null
+  const double* b0f;  // background field averaged over the faces [9][NI][NJ][NK], or null
   double* scratch;    // device address of g_cfl_scratch on this device
   double* out;        // out[0] = dt, out[1] = max|div B|
   int nblocks;
@@ -87,6 +89,12 @@ __device__ void cell_dt_divb(const Args& A, int i, int j, int k, double& dt, dou
   double m1 = b[c] * (x1[i + 1] - xc[0]) / d1 + b[c + s1] * (xc[0] - x1[i]) / d1;
   double m2 = b[n3 + c] * (x2[j + 1] - xc[1]) / d2 + b[n3 + c + s2] * (xc[1] - x2[j]) / d2;
   double m3 = b[2 * n3 + c] * (x3[k + 1] - xc[2]) / d3 + b[2 * n3 + c + 1] * (xc[2] - x3[k]) / d3;
+  // magtot = mags + B0 (src/solver_func.c:345-353)
+  if (A.b0) {
+    m1 += A.b0[c];
+    m2 += A.b0[n3 + c];
+    m3 += A.b0[2 * n3 + c];
+  }
   // get_dt_normal (src/solver_func.c:255-298)
   double rho = g[c], u = g[n3 + c], v = g[2 * n3 + c], w = g[3 * n3 + c], p = g[4 * n3 + c];
   double va = sqrt((m1 * m1 + m2 * m2 + m3 * m3) / rho);
@@ -105,9 +113,24 @@ __device__ void cell_dt_divb(const Args& A, int i, int j, int k, double& dt, dou
   double vol = A.sph ? fabs(1.0 / 3.0 * (pow(x1[i + 1], 3) - pow(x1[i], 3)) *
                             (cos(x2[j + 1]) - cos(x2[j])) * d3)
                      : d1 * d2 * d3;
-  double db = (b[c + s1] * face_area(A, 0, i + 1, j, k) - b[c] * face_area(A, 0, i, j, k)) / vol +
-              (b[n3 + c + s2] * face_area(A, 1, i, j + 1, k) - b[n3 + c] * face_area(A, 1, i, j, k)) / vol +
-              (b[2 * n3 + c + 1] * face_area(A, 2, i, j, k + 1) - b[2 * n3 + c] * face_area(A, 2, i, j, k)) / vol;
+  // face-normal field, plus the face-averaged background normal component
+  // (B0AfaceI/J/K_bn, src/solver_func.c:324-343)
+  double bl[3] = {b[c], b[n3 + c], b[2 * n3 + c]};
+  double bu[3] = {b[c + s1], b[n3 + c + s2], b[2 * n3 + c + 1]};
+  if (A.b0f) {
+    const double* f0 = A.b0f;            // faces normal to i, component i
+    const double* f1 = A.b0f + 4 * n3;   // faces normal to j, component j
+    const double* f2 = A.b0f + 8 * n3;   // faces normal to k, component k
+    bl[0] += f0[c];
+    bu[0] += f0[c + s1];
+    bl[1] += f1[c];
+    bu[1] += f1[c + s2];
+    bl[2] += f2[c];
+    bu[2] += f2[c + 1];
+  }
+  double db = (bu[0] * face_area(A, 0, i + 1, j, k) - bl[0] * face_area(A, 0, i, j, k)) / vol +
+              (bu[1] * face_area(A, 1, i, j + 1, k) - bl[1] * face_area(A, 1, i, j, k)) / vol +
+              (bu[2] * face_area(A, 2, i, j, k + 1) - bl[2] * face_area(A, 2, i, j, k)) / vol;
   divb = fabs(db);
 }
 
@@ -182,10 +205,17 @@ double* g_addr[64] = {};
 }  // namespace
 
 extern "C" int gop_cfl_dt_noalloc(const gop_desc* desc, const double* gas, const double* face_b,
-                                  double* out, void* stream) {
+                                  const double* b0, const double* b0_face, double* out,
+                                  void* stream) {
   int rc = gop::check_desc(desc);
   if (rc) return rc;
   if (!gas || !face_b || !out) return gop::set_error(GOP_EINVAL, "gop_cfl_dt_noalloc: NULL array");
+  if ((b0 == nullptr) != (b0_face == nullptr))
+    return gop::set_error(GOP_EINVAL, "gop_cfl_dt_noalloc: b0 and b0_face go together");
+  // ring-averaged grids take the CFL length of their pole rows from the
+  // ring average (get_dt_ring), which this call does not compute
+  if (desc->ring_average)
+    return gop::set_error(GOP_EINVAL, "gop_cfl_dt_noalloc: grids with the pole ring average are not supported");
   if (desc->ni > kMaxN || desc->nj > kMaxN || desc->nk > kMaxN)
     return gop::set_error(GOP_EINVAL,
                           "gop_cfl_dt_noalloc: grid %dx%dx%d exceeds the static scratch limit of %d "
@@ -222,6 +252,8 @@ extern "C" int gop_cfl_dt_noalloc(const gop_desc* desc, const double* gas, const
   A.ca2 = A.ca * A.ca;
   A.gas = gas;
   A.fb = face_b;
+  A.b0 = b0;
+  A.b0f = b0_face;
   A.scratch = scratch;
   A.out = out;
   const double* xs[3] = {desc->x1, desc->x2, desc->x3};

@@ -183,26 +183,36 @@ int64_t gop_kernel_launches(void);
 
 /* No counterpart in the reference: GAMERA-OP has no GPU and no allocation
  * constraints.  This is the one entry point for callers that must not
- * allocate device memory -- e.g. code between the capture calls of a CUDA
- * graph, where cudaMalloc is not capturable, or a serving loop whose device
- * memory was reserved at start-up and may not grow.
+ * allocate device memory -- a serving loop whose device memory was
+ * reserved at start-up and may not grow (cudaMalloc there can fail, and it
+ * and cudaFree wait for work running on the device), or a host program that
+ * owns every device buffer itself and hands the library only pointers.
  *
  * gas (6 fields) and face_b (3 fields) are DEVICE pointers in the layout of
- * gop_upload; out is a device pointer to 2 doubles that receives the CFL dt
- * (get_dt_normal, src/solver_func.c:255-298) and max|div B|
- * (src/solver_func.c:324-343) over the active cells.  Asynchronous on
- * `stream` (cudaStream_t as void*); it calls no cudaMalloc/cudaFree.
+ * gop_upload.  b0 (3 fields, B0 at the cell centroid) and b0_face (9
+ * fields, field 3d+c = component c averaged over the faces normal to axis
+ * d) describe a background field in the layout gop_set_background takes,
+ * as DEVICE pointers; both NULL for none.  out is a device pointer to 2
+ * doubles: the CFL time step over the active cells (CFL over the sum, over
+ * the three axes, of the fast signal speed -- |v| plus the fast
+ * magnetosonic speed with the Boris-limited Alfven speed of the cell's total
+ * field -- divided by the cell's length along that axis) and the largest
+ * |div B| of the cell-integrated total face field.  Asynchronous on `stream`
+ * (cudaStream_t as void*); it calls no cudaMalloc/cudaFree.  Grids with
+ * ring_average set are rejected with GOP_EINVAL.
  *
  * Its scratch is one file-scope device array of GOP_NOALLOC_SCRATCH_DOUBLES
  * doubles (64 KiB), held by every GPU that loads the library until exit, so
  * grids are limited to GOP_NOALLOC_MAX_N active cells per axis (larger ones
  * are rejected with GOP_EINVAL).  The first call on a device looks up that
- * array's device address; make it before any stream capture.  All calls
- * share the array: calls whose kernels overlap on the GPU race. */
+ * array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  The coordinate arrays of desc are copied into it
+ * from the host on `stream` at every call.  All calls share the array:
+ * calls whose kernels overlap on the GPU race. */
 #define GOP_NOALLOC_MAX_N 1024
 #define GOP_NOALLOC_SCRATCH_DOUBLES 8192
 int gop_cfl_dt_noalloc(const gop_desc *desc, const double *gas, const double *face_b,
-                       double *out, void *stream);
+                       const double *b0, const double *b0_face, double *out, void *stream);
 
 /* ---- host-only problem setup (no device work) ------------------------ */
 

@@ -19,7 +19,9 @@
  *   GOP_RING     1: doRingAverage = 1 (the pole ring average)
  *   GOP_CA       Boris "speed of light" CA               (default 10)
  *   blast:  GOP_RHO, GOP_P_IN, GOP_P_OUT, GOP_RADIUS, GOP_CENTER "x,y,z",
- *           GOP_B "b1,b2,b3" (uniform face field)
+ *           GOP_B "b1,b2,b3" (uniform face field), GOP_RHO_IN (density
+ *           inside the radius, default GOP_RHO: below the density floor
+ *           it drives the positivity floors of check_positivity)
  *   loop_sph: GOP_V "vx,vy,vz" (Cartesian), GOP_RHO, GOP_P, GOP_LOOP
  *           "xc,yc,R,A0"
  *   GOP_PS   f: the entropy channel p_S = f * p in every initialised cell
@@ -295,6 +297,7 @@ void problem_init() {
     double rho = env_d("GOP_RHO", 1.0);
     double p_in = env_d("GOP_P_IN", 10.0), p_out = env_d("GOP_P_OUT", 0.1);
     double rad = env_d("GOP_RADIUS", 0.1);
+    double rho_in = env_d("GOP_RHO_IN", rho);
     for (int s = 0; s < NS1; s++)
       for (int i = is; i <= ie; i++)
         for (int j = js; j <= je; j++)
@@ -302,7 +305,7 @@ void problem_init() {
             double dx = x1c[i][j][k] - c[0], dy = x2c[i][j][k] - c[1],
                    dz = x3c[i][j][k] - c[2];
             double r = sqrt(dx * dx + dy * dy + dz * dz);
-            gas[s][gas_rho][i][j][k] = rho;
+            gas[s][gas_rho][i][j][k] = r < rad ? rho_in : rho;
             gas[s][gas_v1][i][j][k] = 0.0;
             gas[s][gas_v2][i][j][k] = 0.0;
             gas[s][gas_v3][i][j][k] = 0.0;

@@ -102,6 +102,41 @@ class RefRun:
         return st
 
 
+def _coords(dims):
+    from itertools import product
+    return list(product(*(range(d) for d in dims)))
+
+
+def stitch(parts: list, dims: tuple, n: tuple) -> dict:
+    """One dump of a run on a ``dims`` process grid, from the per-rank dumps
+    ``parts`` (in rank order, the last axis fastest): every rank's active
+    cells and its lower faces, the upper boundary faces from the last rank
+    along each axis.  Ghost layers of the whole grid are left zero (a GPU
+    instance fills them from its own boundary kinds)."""
+    from itertools import product
+    nl = tuple(n[a] // dims[a] for a in range(3))
+    N = tuple(v + 2 * NG + 1 for v in n)
+    out = {k: v for k, v in parts[0].items() if k not in ("gas", "gem")}
+    for key in ("gas", "gem"):
+        if key not in parts[0]:
+            continue
+        lead = parts[0][key].shape[:-3]
+        arr = np.zeros(lead + N)
+        for r, c in enumerate(product(*(range(d) for d in dims))):
+            src = parts[r][key]
+            sl_g, sl_l = [], []
+            for a in range(3):
+                top = 1 if c[a] == dims[a] - 1 else 0  # the upper boundary face
+                sl_g.append(slice(NG + c[a] * nl[a], NG + (c[a] + 1) * nl[a] + top))
+                sl_l.append(slice(NG, NG + nl[a] + top))
+            arr[(Ellipsis,) + tuple(sl_g)] = src[(Ellipsis,) + tuple(sl_l)]
+        out[key] = arr
+    return out
+
+
+NG = 4
+
+
 def run(
     n: tuple,
     steps: int,
@@ -115,22 +150,26 @@ def run(
     timeout: float | None = None,
     exe: str | os.PathLike | None = None,
     output_interval: float = 1e30,
+    dims: tuple = (1, 1, 1),
 ) -> RefRun:
     """Runs ``steps`` steps of the reference on an ``n=(ni,nj,nk)`` grid.
 
     With ``keep_output`` the step-0 dump and the final dump are read back;
     otherwise writes are discarded (used for timing) and the shim reports the
-    wall time of the step loop.
+    wall time of the step loop.  ``dims`` > (1, 1, 1) runs the reference as
+    that many ranks (the MPI stand-in forks them, one process per rank) on a
+    ``dims`` process grid; the per-rank dumps are stitched back into one.
     """
     exe = Path(exe) if exe else binary(coord, flavor)
     if not exe.exists():
         raise FileNotFoundError(f"{exe} is not built (make -C oracle reference)")
     ni, nj, nk = n
+    nranks = dims[0] * dims[1] * dims[2]
     tmp = tempfile.mkdtemp(prefix="gop_ref_")
     try:
         cfg = (
             f"ni_global: {ni}\nnj_global: {nj}\nnk_global: {nk}\n"
-            "proc_dims_i: 1\nproc_dims_j: 1\nproc_dims_k: 1\n"
+            f"proc_dims_i: {dims[0]}\nproc_dims_j: {dims[1]}\nproc_dims_k: {dims[2]}\n"
             f"Nt: {steps}\ntime_stop: {time_stop!r}\n"
             f"output_interval: {output_interval!r}\n"
             "x_Norm: 1.0\nu_Norm: 1.0\nrho_Norm: 1.0\n"
@@ -138,23 +177,41 @@ def run(
         Path(tmp, "config.yaml").write_text(cfg)
         e = dict(os.environ)
         e.update({"OMP_NUM_THREADS": str(threads), "GOP_PROBLEM": problem,
-                  "GOP_SHIM_TIMING": "1"})
+                  "GOP_SHIM_TIMING": "1", "GOP_SHIM_RANKS": str(nranks)})
         if not keep_output:
             e["GOP_H5_DISCARD"] = "1"
         e.update(env or {})
-        p = subprocess.run([str(exe), "config.yaml"], cwd=tmp, env=e,
-                           capture_output=True, text=True, timeout=timeout)
-        if p.returncode != 0:
-            raise RuntimeError(f"reference run failed ({p.returncode}): {p.stderr[-2000:]}")
+        # its own session, so a timeout takes down every rank
+        proc = subprocess.Popen([str(exe), "config.yaml"], cwd=tmp, env=e, text=True,
+                                stdout=subprocess.PIPE, stderr=subprocess.PIPE,
+                                start_new_session=True)
+        try:
+            _, err = proc.communicate(timeout=timeout)
+        except subprocess.TimeoutExpired:
+            os.killpg(proc.pid, 9)
+            proc.communicate()
+            raise
+        if proc.returncode != 0:
+            raise RuntimeError(f"reference run failed ({proc.returncode}): {err[-2000:]}")
         files = sorted(f for f in os.listdir(tmp) if f.startswith("mhd_") and f.endswith(".h5"))
-        dumps = [read_raw(Path(tmp, f)) for f in files] if keep_output else []
-        rr = RefRun(dumps=dumps, stderr=p.stderr, files=files)
-        m = re.search(r"GOP_SHIM_TIMING calls=(\d+) t1=([\d.]+) tlast=([\d.]+)", p.stderr)
+        dumps = []
+        if keep_output:
+            if nranks == 1:
+                dumps = [read_raw(Path(tmp, f)) for f in files]
+            else:
+                # mhd_II-JJ-KK_SEQ.h5: group the ranks' files by output number
+                seqs = sorted({f.rsplit("_", 1)[1] for f in files})
+                for q in seqs:
+                    parts = [read_raw(Path(tmp, f"mhd_{c[0]:02d}-{c[1]:02d}-{c[2]:02d}_{q}"))
+                             for c in _coords(dims)]
+                    dumps.append(stitch(parts, dims, n))
+        rr = RefRun(dumps=dumps, stderr=err, files=files)
+        m = re.search(r"GOP_SHIM_TIMING calls=(\d+) t1=([\d.]+) tlast=([\d.]+)", err)
         if m:
             calls = int(m.group(1))
             rr.wall_steps = calls - 2
             rr.wall_seconds = float(m.group(3)) - float(m.group(2))
-        m = re.search(r"GOP_SHIM_TIMES ([\d. ]+)", p.stderr)
+        m = re.search(r"GOP_SHIM_TIMES ([\d. ]+)", err)
         if m:
             # call 0 = initial dt, call n = start of step n
             rr.step_starts = [float(v) for v in m.group(1).split()][1:]

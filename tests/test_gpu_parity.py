@@ -130,6 +130,36 @@ def test_orszag_tang_256x256x4_100_steps_matches_reference_binary(gop):
     assert st["divb_max"] < 1e-10
 
 
+def test_blast_c2_length_64cube_200_steps_matches_reference_binary(gop):
+    """The C2 blast (p = 10 inside r < 0.1 of the centre, 0.1 outside,
+    B = (1/sqrt2, 1/sqrt2, 0), periodic) for C2's full 200 steps, at 64^3:
+    the largest cube GAMERA-OP's strict FP64 build (one thread) finishes in a
+    few minutes.  Both start from the reference's step-0 state; relative L1
+    <= 1e-10 per variable, equal simulated time, div B at round-off."""
+    ref_run = pytest.importorskip("ref_run")
+    if not ref_run.available("cart", "strict"):
+        pytest.skip("oracle/_ref/ref_cart_strict not built")
+    n = (64, 64, 64)
+    ref = ref_run.run(n, 200, problem="blast",
+                      env={"GOP_BC": "pppppp", "GOP_DOMAIN": "-0.5,0.5,-0.5,0.5,-0.5,0.5"},
+                      timeout=3000)
+    s0, s1 = ref.state(0), ref.state(-1)
+    x = [gop.grid_uniform(m, -0.5, 0.5) for m in n]
+    inst = gop.Instance(n, *x)
+    W0 = np.stack([s0[k] for k in ("rho", "v1", "v2", "v3", "p", "pS")])
+    B0 = np.stack([s0[k] for k in ("bi", "bj", "bk")])
+    inst.upload(W0, B0)
+    inst.prepare()
+    inst.step(200)
+    d = inst.download(("gas", "face_b"))
+    Wr = np.stack([s1[k] for k in ("rho", "v1", "v2", "v3", "p", "pS")])
+    Br = np.stack([s1[k] for k in ("bi", "bj", "bk")])
+    compare(n, d["gas"], d["face_b"], Wr, Br, TOL_FP64, "blast 64^3 x200 vs reference")
+    st = inst.stats()
+    assert math.isclose(st["time"], s1["time"], rel_tol=1e-12)
+    assert st["divb_max"] < 1e-10
+
+
 def test_blast_3d_matches_oracle(gop, oracle_mod):
     n = (32, 32, 32)
     x = [gop.grid_uniform(m, -0.5, 0.5) for m in n]
