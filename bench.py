@@ -37,6 +37,7 @@ for p in (ROOT / "gamera-op_b200", ROOT / "oracle"):
 METRIC = "Mcell-updates/s vs plain FP64 GPU at fixed L1 err; %HBM peak; p50/p99 lat"
 UNIT = "Mcell-updates/s"
 BYTES_PER_CELL_UPDATE = 216  # algorithmic bytes of one cell-update (FP64)
+REF_BUDGET_S = 120  # seconds of timed steps the reference arm may spend
 GROUP_LAUNCHES = {"ab2": 1, "c2c": 3, "emf": 3, "flux": 3, "update": 1}
 # thread-block shapes the library's autotuner chooses from (gop_autotune)
 BLOCK_CANDIDATES = ["32x4x2", "32x8x1", "32x1x8", "32x2x4", "64x2x2", "64x4x1", "64x1x4",
@@ -242,16 +243,20 @@ def run_reference(args, rank):
                f"{avail / 2**30:.0f} GiB available")
     dims = rank_dims(cores, n)
     ranks = dims[0] * dims[1] * dims[2]
-    r = ref_run.run(n, args.warmup + args.steps + 1, problem="blast", flavor="release",
+    cells = n[0] * n[1] * n[2]
+    # a bounded sample of the K steps: about REF_BUDGET_S seconds of steps at
+    # a conservative 0.4 M cell-updates/s per rank
+    est = cells / (ranks * 0.4e6)
+    steps = max(3, min(args.steps, int(REF_BUDGET_S / est)))
+    r = ref_run.run(n, args.warmup + steps + 1, problem="blast", flavor="release",
                     keep_output=False, threads=1, dims=dims,
                     env={"GOP_SHIM_TIMING": "2", "GOP_BC": "pppppp",
                          "GOP_DOMAIN": "-0.5,0.5,-0.5,0.5,-0.5,0.5"}, timeout=3000)
     starts = r.step_starts
     w = args.warmup
-    t = starts[w + args.steps] - starts[w]
-    cells = n[0] * n[1] * n[2]
-    v = cells * args.steps / t / 1e6
-    durs = np.diff(starts[w:w + args.steps + 1]) * 1e3
+    t = starts[w + steps] - starts[w]
+    v = cells * steps / t / 1e6
+    durs = np.diff(starts[w:w + steps + 1]) * 1e3
     cfg = {"workload": f"blast3d_periodic_{args.n}^3_{args.precision}",
            "grid": list(full),
            "problem": "blast p_in=10 p_out=0.1 r=0.1 B=(1/sqrt2,1/sqrt2,0) gamma=5/3 CFL=0.3",
@@ -261,15 +266,16 @@ def run_reference(args, rank):
     if n != full:
         cfg["sample_grid"] = list(n)
         cfg["note"] = f"each step timed at {n[0]}^3 instead of {args.n}^3: {why}"
+    cfg["timed_steps"] = steps
     line.update({
-        "value": round(v, 4), "ms_per_step": round(t / args.steps * 1e3, 3),
+        "value": round(v, 4), "ms_per_step": round(t / steps * 1e3, 3),
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": cfg,
         "latency_ms": {"p50": round(float(np.percentile(durs, 50)), 3),
                        "p99": round(float(np.percentile(durs, 99)), 3)},
         "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": ranks, "kind": "reference",
-                         "sample": f"blast {n[0]}^3, {args.steps} steps after {w} warm-up, "
-                                   f"{ranks} ranks x 1 thread, Release flags"},
+                         "sample": f"blast {n[0]}^3, {steps} of the {args.steps} steps timed after "
+                                   f"{w} warm-up, {ranks} ranks x 1 thread, Release flags"},
         "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     })
     print(json.dumps(line))

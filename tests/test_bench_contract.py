@@ -35,8 +35,10 @@ def test_reference_arm_prints_one_contract_line():
     if not (ROOT / "oracle" / "_ref" / "ref_cart_release_v3").exists():
         pytest.skip("oracle/_ref not built")
     # at least 3 warm-up steps (a smaller --warmup is raised to 3)
+    # a 32^3 grid keeps the CPU suite short; the default is the workload's 256^3
     out = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "2",
-                          "--warmup", "1"], cwd=ROOT, capture_output=True, text=True, timeout=600)
+                          "--warmup", "1", "--n", "32"], cwd=ROOT, capture_output=True, text=True,
+                         timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
     assert len(lines) == 1
@@ -48,6 +50,18 @@ def test_reference_arm_prints_one_contract_line():
     assert d["cpu_baseline"]["value"] == d["value"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
-    # the same workload as the CUDA arm's default line, timed on a bounded sample
-    assert d["config"]["workload"] == "blast3d_periodic_256^3_fp64"
-    assert d["config"]["sample_grid"] == [64, 64, 64]
+    # the workload's own grid, as ranks of one thread each (README mode)
+    assert d["config"]["workload"] == "blast3d_periodic_32^3_fp64"
+    assert d["config"]["grid"] == [32, 32, 32] and "sample_grid" not in d["config"]
+    dims = d["config"]["process_grid"]
+    assert d["config"]["threads_per_rank"] == 1
+    assert d["config"]["ranks"] == dims[0] * dims[1] * dims[2] == d["cpu_baseline"]["cores"]
+
+
+def test_rank_grid_divides_the_workload():
+    import bench
+    for cores in (1, 3, 8, 16, 24, 64, 112):
+        for n in ((256, 256, 256), (128, 128, 128), (32, 32, 32)):
+            dims = bench.rank_dims(cores, n)
+            r = dims[0] * dims[1] * dims[2]
+            assert r <= max(cores, 1) and all(n[a] % dims[a] == 0 for a in range(3))
