@@ -686,9 +686,25 @@ def _run_to(gop, torch, inst, steps, time_stop):
     return a.elapsed_time(b), inst.stats()["steps"] - s0
 
 
+def _perturbed(gop, make, rel=1e-15, seed=7):
+    """An FP64 instance whose initial density differs from make()'s by a
+    seeded relative perturbation of about `rel` per cell (round-off level)."""
+    inst = make(gop.PREC_FP64)
+    d = inst.download(("gas", "face_b"))
+    rng = np.random.default_rng(seed)
+    gas = d["gas"].copy()
+    gas[0] *= 1.0 + rel * rng.uniform(-1.0, 1.0, size=gas[0].shape)
+    inst.upload(gas, d["face_b"])
+    return inst
+
+
 def _single_pair(args, gop, torch, local, make, n, t_end, workload, extra):
     """FP64 to t_end, then the mixed path for the same number of steps; the
-    mixed result is compared with the FP64 one."""
+    mixed result is compared with the FP64 one.  A third run, FP64 again from
+    an initial density perturbed at round-off level (1e-15 relative), shows
+    how far two FP64 solutions of the same problem drift apart by then: the
+    floor below which the mixed path's error is the problem's sensitivity,
+    not its precision."""
     from gop import accuracy
     warm = make(gop.PREC_FP64)
     warm.prepare()
@@ -708,10 +724,16 @@ def _single_pair(args, gop, torch, local, make, n, t_end, workload, extra):
     which = ("gas", "face_b", "mags")
     a, b = mx.download(which), f64.download(which)
     errs = accuracy.rel_l1(n, a, b)
+    pt = _perturbed(gop, make)
+    pt.prepare()
+    _run_to(gop, torch, pt, steps, 1e300)
+    c = pt.download(which)
+    errs_pt = accuracy.rel_l1(n, c, b)
     sl = tuple(slice(4, 4 + m) for m in n)
-    bm = lambda d: np.sqrt(sum(d["mags"][c][sl] ** 2 for c in range(3)))
-    ba, bb = bm(a), bm(b)
+    bm = lambda d: np.sqrt(sum(d["mags"][k][sl] ** 2 for k in range(3)))
+    ba, bb, bc = bm(a), bm(b), bm(c)
     l1_bmag = float(np.abs(ba - bb).sum() / max(np.abs(bb).sum(), 1e-300))
+    l1_bmag_pt = float(np.abs(bc - bb).sum() / max(np.abs(bb).sum(), 1e-300))
     st64, stmx = f64.stats(), mx.stats()
     rate = lambda ms, k: round(cells * k / (ms / 1e3) / 1e6, 3)
     line = {
@@ -728,10 +750,13 @@ def _single_pair(args, gop, torch, local, make, n, t_end, workload, extra):
         "accuracy_vs_fp64": {"rel_l1": errs, "l1_bmag": l1_bmag, "l1_rho": errs["rho"],
                              "max_divb_mixed": stmx["divb_max"], "time_mixed": stmx["time"],
                              "tolerance": 1e-5},
+        "fp64_sensitivity": {"what": "FP64 from a 1e-15 relative density perturbation vs FP64",
+                             "rel_l1": errs_pt, "l1_bmag": l1_bmag_pt, "l1_rho": errs_pt["rho"]},
         "gpu_launches": int(launches), "clocks": clk,
     }
     f64.close()
     mx.close()
+    pt.close()
     return line
 
 
