@@ -6,7 +6,8 @@
  * reference's whole host side -- main (src/main.c), config.yaml, problem
  * hooks, geometry and weights, HDF5 output -- and moves the time loop onto
  * the GPU through the C ABI of include/gamera_op.h.  The state stays on the
- * device between output times; at every output time (and once at the end)
+ * device, which steps on its own up to the next host event (a dump time, a
+ * log time or time_stop); at every output time (and once at the end)
  * the 18 store slots of gas[0] and gem are copied back into the host arrays
  * and written by the reference's own dump_data_hdf5 (src/hdf5_io.c:353-523),
  * so the per-step files keep their layout.
@@ -145,11 +146,30 @@ int solve(int nt) {
   dt0 = st.dt0;
 
   time_sim_start = time_sim;
-  for (int n = 1; n <= nt; n++) {
+  /* The reference needs the host only when time_sim reaches a dump or a log
+   * threshold or passes time_stop (src/solver_solve.c:508-525).  So the
+   * device steps on its own up to the first such event: gop_step stops after
+   * the first step that takes time past its limit, and a limit just below a
+   * threshold (nextafter) stops it at the first step reaching it, where the
+   * host then acts exactly as the reference does after that step. */
+  int n = 0;
+  while (n < nt) {
+    double stop = time_stop;
+    const double t_dump = output_interval * (hdf_seq_num + 1);
+    const double t_log = 0.1 * output_interval * (log_seq_num);
+    if (nextafter(t_dump, -INFINITY) < stop) stop = nextafter(t_dump, -INFINITY);
+    if (nextafter(t_log, -INFINITY) < stop) stop = nextafter(t_log, -INFINITY);
+    /* an event already due (time_sim past the limit: the step counter's
+     * first log, or a threshold the last step crossed twice over) happens
+     * after the very next step */
+    const int due = time_sim > stop;
     double t = 0.0;
-    rc = gop_step(h, 1, 1e300, &t);
+    const int64_t before = st.steps;
+    rc = gop_step(h, due ? 1 : nt - n, due ? 1e300 : stop, &t);
     if (rc) return gop_fail(h, "gop_step", rc);
     gop_get_stats(h, &st);
+    if (st.steps == before) break; /* the limit was already behind: nothing ran */
+    n += (int)(st.steps - before);
     time_sim = t;
     dt = st.dt;
     dt0 = st.dt0;

@@ -83,6 +83,7 @@ class RefRun:
     wall_seconds: float = 0.0
     files: list = field(default_factory=list)
     step_starts: list = field(default_factory=list)
+    log: str = ""  # the run's log files (rank order), where log_info writes
 
     def state(self, idx: int = -1) -> dict:
         """Primitive state and face B (ghost-extended, reference layout
@@ -205,7 +206,9 @@ def run(
                     parts = [read_raw(Path(tmp, f"mhd_{c[0]:02d}-{c[1]:02d}-{c[2]:02d}_{q}"))
                              for c in _coords(dims)]
                     dumps.append(stitch(parts, dims, n))
-        rr = RefRun(dumps=dumps, stderr=err, files=files)
+        logs = sorted(f for f in os.listdir(tmp) if f.endswith(".log"))
+        rr = RefRun(dumps=dumps, stderr=err, files=files,
+                    log="".join(Path(tmp, f).read_text(errors="replace") for f in logs))
         m = re.search(r"GOP_SHIM_TIMING calls=(\d+) t1=([\d.]+) tlast=([\d.]+)", err)
         if m:
             calls = int(m.group(1))

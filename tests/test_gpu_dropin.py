@@ -82,3 +82,26 @@ def test_dropin_writes_outputs_at_the_reference_times():
     for a, b in zip(gpu.dumps, ref.dumps):
         assert abs(float(a["time_sim"][0]) - float(b["time_sim"][0])) <= 1e-12
         _compare_dumps(a, b, (16, 16, 16), 1e-10)
+
+
+def test_dropin_stops_and_logs_at_the_reference_steps():
+    """The drop-in steps on the device up to the next host event (dump time,
+    log time, time_stop) instead of returning to the host every step; the
+    reference's status lines (step number and time) and its stop come out at
+    the same steps."""
+    import re
+    _need("ref_cart_strict", "ref_cart_gpu")
+    kw = dict(problem="blast", coord="cart", env={"GOP_BC": "pppppp"}, timeout=600,
+              output_interval=0.05, time_stop=0.06)
+    ref = ref_run.run((16, 16, 16), 1000, **kw)
+    gpu = ref_run.run((16, 16, 16), 1000, exe=ref_run.REF_DIR / "ref_cart_gpu", **kw)
+    pat = re.compile(r"Status at step (\d+): rank \d+, Time ([\d.]+)")
+    a, b = pat.findall(gpu.log), pat.findall(ref.log)
+    steps = [int(s) for s, _ in b]
+    assert len(b) >= 3 and max(y - x for x, y in zip(steps, steps[1:])) > 1
+    assert [s for s, _ in a] == [s for s, _ in b]
+    for (_, ta), (_, tb) in zip(a, b):
+        assert abs(float(ta) - float(tb)) <= 1e-12
+    assert gpu.files == ref.files
+    assert abs(gpu.state(-1)["time"] - ref.state(-1)["time"]) <= 1e-12
+    assert ref.state(-1)["time"] > 0.06 and len(ref.files) == 3
