@@ -18,6 +18,7 @@ SOURCES = [
     PKG / "csrc" / "gop_sweep.cu",
     PKG / "csrc" / "gop_noalloc.cu",
     PKG / "csrc" / "gop_init.cu",
+    PKG / "csrc" / "gop_bgdev.cu",
     PKG / "csrc" / "gop_ring.cu",
     PKG / "host" / "gop_problems.c",
     PKG / "host" / "gop_background.c",
@@ -25,7 +26,7 @@ SOURCES = [
 HEADERS = [ROOT / "include" / "gamera_op.h", PKG / "csrc" / "gop_device.cuh",
            PKG / "csrc" / "gop_kernels.h", PKG / "csrc" / "gop_internal.h",
            PKG / "csrc" / "gop_stage.cuh", PKG / "csrc" / "gop_tma.cuh",
-           PKG / "csrc" / "gop_fields.h"]
+           PKG / "csrc" / "gop_fields.h", PKG / "csrc" / "gop_bgfield.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -406,6 +406,24 @@ struct gop_instance {
   int64_t prof_n[NGROUP] = {};
 };
 
+// the background block (BG_NF fields of doubles), allocated at first use and
+// zeroed
+static int alloc_background(gop_instance* h) {
+  const Params& P = h->P;
+  if (!h->bg) {
+    cudaError_t e = cudaMallocAsync((void**)&h->bg, (size_t)P.fs * BG_NF * sizeof(double), h->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      h->bg = nullptr;
+      return fail(GOP_ENOMEM, "background allocation failed: %s", cudaGetErrorString(e));
+    }
+    h->bytes += (size_t)P.fs * BG_NF * sizeof(double);
+  }
+  CK(cudaMemsetAsync(h->bg, 0, (size_t)P.fs * BG_NF * sizeof(double), h->st));
+  return GOP_OK;
+}
+
 static cudaEvent_t take_event(gop_instance* h) {
   cudaEvent_t e = nullptr;
   if (!h->pool.empty()) {
@@ -690,17 +708,8 @@ int gop_set_background(gop_instance* h, const double* b0, const double* lorentz,
     CK(cudaStreamSynchronize(h->st));
     return GOP_OK;
   }
-  if (!h->bg) {
-    cudaError_t e = cudaMallocAsync((void**)&h->bg, (size_t)P.fs * BG_NF * sizeof(double), h->st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      h->bg = nullptr;
-      return fail(GOP_ENOMEM, "background allocation failed: %s", cudaGetErrorString(e));
-    }
-    h->bytes += (size_t)P.fs * BG_NF * sizeof(double);
-  }
-  CK(cudaMemsetAsync(h->bg, 0, (size_t)P.fs * BG_NF * sizeof(double), h->st));
+  int rc = alloc_background(h);
+  if (rc) return rc;
   const size_t ref = (size_t)P.N[0] * P.N[1] * P.N[2];
   // through the staging buffer (6 fields) in groups of 3
   const double* src[8] = {b0, lorentz, b0_face, b0_face + 3 * ref, b0_face + 6 * ref,
@@ -714,6 +723,44 @@ int gop_set_background(gop_instance* h, const double* b0, const double* lorentz,
   CK(cudaStreamSynchronize(h->st));
   CK(cudaGetLastError());
   P.bg = h->bg;
+  return GOP_OK;
+}
+
+int gop_set_background_device(gop_instance* h, const gop_background* bg) {
+  if (!h || !bg) return fail(GOP_EINVAL, "NULL argument");
+  if (bg->kind != GOP_BG_UNIFORM && bg->kind != GOP_BG_DIPOLE)
+    return fail(GOP_EINVAL, "unknown background kind %d", bg->kind);
+  Params& P = h->P;
+  drop_step_graph(h);  // the captured step has the other kernel set
+  h->prepared = false;
+  int rc = alloc_background(h);
+  if (rc) return rc;
+  // the work arrays (>= 12 fields of doubles) are free until gop_prepare
+  launch_background(P, *bg, h->d.coord == GOP_COORD_SPHERICAL ? 1 : 0, h->bg, (double*)h->work,
+                    h->st);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->st));
+  P.bg = h->bg;
+  return GOP_OK;
+}
+
+int gop_get_background(gop_instance* h, double* b0, double* lorentz, double* b0_face,
+                       double* b0_edge) {
+  if (!h) return fail(GOP_EINVAL, "instance is NULL");
+  if (!h->bg) return fail(GOP_ESTATE, "the instance has no background field");
+  const Params& P = h->P;
+  const size_t ref = (size_t)P.N[0] * P.N[1] * P.N[2];
+  double* dst[8] = {b0, lorentz, b0_face, b0_face ? b0_face + 3 * ref : nullptr,
+                    b0_face ? b0_face + 6 * ref : nullptr, b0_edge,
+                    b0_edge ? b0_edge + 3 * ref : nullptr, b0_edge ? b0_edge + 6 * ref : nullptr};
+  const int src[8] = {BG_B0, BG_LOR, BG_FACE, BG_FACE + 3, BG_FACE + 6,
+                      BG_EDGE, BG_EDGE + 3, BG_EDGE + 6};
+  for (int g = 0; g < 8; g++) {
+    if (!dst[g]) continue;
+    launch_to_ref(P, 3, h->bg + (size_t)src[g] * P.fs, h->staging, h->st);
+    CK(cudaMemcpyAsync(dst[g], h->staging, 3 * ref * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  }
+  CK(cudaStreamSynchronize(h->st));
   return GOP_OK;
 }
 

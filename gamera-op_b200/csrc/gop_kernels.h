@@ -113,6 +113,10 @@ void launch_mags(const Params& P, const double* B, double* out, cudaStream_t st)
 template <typename R>
 void launch_pole_emf(const Params& P, const Work<R>& w, cudaStream_t st);
 void launch_ring_average(const Params& P, double* scratch, cudaStream_t st);
+// background field B0 of a built-in kind into the background block out
+// (BG_NF fields, zero beforehand); aux: 12 fields of doubles of scratch
+void launch_background(const Params& P, const gop_background& bg, int sph, double* out, double* aux,
+                       cudaStream_t st);
 // problem p's initial state in buffer 0 (cells, face field; ghosts left for
 // the ghost fill); scratch: 3 fields of doubles for the edge integrals
 void launch_problem_init(const Params& P, const gop_problem& p, int sph, double* scratch,

@@ -100,6 +100,8 @@ def lib():
         L.gop_problem_init_device.argtypes = [vp, C.POINTER(Problem)]
         L.gop_set_background.argtypes = [vp, _dp, _dp, _dp, _dp]
         L.gop_background_init.argtypes = [C.POINTER(Desc), C.POINTER(Background), _dp, _dp, _dp, _dp]
+        L.gop_set_background_device.argtypes = [vp, C.POINTER(Background)]
+        L.gop_get_background.argtypes = [vp, _dp, _dp, _dp, _dp]
         L.gop_autotune.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
         L.gop_set_profiling.argtypes = [vp, C.c_int]
         L.gop_set_sweep.argtypes = [vp, C.c_int]
@@ -240,6 +242,20 @@ class Instance:
         arr = [_contig(fields[k], self.shape(nf)) for k, nf in
                (("b0", 3), ("lorentz", 3), ("b0_face", 9), ("b0_edge", 9))]
         _check(lib().gop_set_background(self._h, *[_ptr(a) for a in arr]))
+
+    def set_background_device(self, kind: int, b=(0.0, 0.0, 0.0), moment=1.0):
+        """Builds a built-in background field on the device, straight into
+        the instance (gop_set_background_device); prepare must follow."""
+        bg = Background(kind, (C.c_double * 3)(*b), moment)
+        _check(lib().gop_set_background_device(self._h, C.byref(bg)))
+
+    def get_background(self) -> dict:
+        """The instance's background field in the layout of background_fields."""
+        out = {"b0": np.zeros(self.shape(3)), "lorentz": np.zeros(self.shape(3)),
+               "b0_face": np.zeros(self.shape(9)), "b0_edge": np.zeros(self.shape(9))}
+        _check(lib().gop_get_background(self._h, _ptr(out["b0"]), _ptr(out["lorentz"]),
+                                        _ptr(out["b0_face"]), _ptr(out["b0_edge"])))
+        return out
 
     def upload(self, gas, face_b, gas_p=None, face_b_p=None, time=0.0, dt0=0.0):
         gas = _contig(gas, self.shape(6))

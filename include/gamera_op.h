@@ -285,6 +285,19 @@ typedef struct {
   double moment;     /* dipole: scale of the reference's unit dipole */
 } gop_background;
 
+/* The same for one of the built-in backgrounds computed on the device,
+ * straight into the instance's background block (the work of
+ * gop_background_init, which takes seconds on the host for a large dipole
+ * grid, without the host arrays or their upload); gop_prepare must follow.
+ * The arrays agree with gop_background_init's to the last bits of the
+ * device's pow, sin and cos. */
+int gop_set_background_device(gop_instance *h, const gop_background *bg);
+
+/* Copies the instance's background field back in gop_set_background's
+ * layout (any pointer may be NULL); GOP_ESTATE without a background. */
+int gop_get_background(gop_instance *h, double *b0, double *lorentz, double *b0_face,
+                       double *b0_edge);
+
 /* set_background_field on the host for one of the built-in backgrounds (no
  * volume source, as in every reference problem): the 12x12 Gauss face
  * averages with the metric scale factors, the 12-point edge averages and

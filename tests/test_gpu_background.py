@@ -141,3 +141,55 @@ def test_background_arguments_go_together(gop):
     inst.set_background(bgf)
     inst.set_background(None)  # removing it again is allowed
     inst.close()
+
+
+DEV_CASES = [
+    dict(id="cart_uniform", n=(20, 16, 12), coord="cart", dom=(-0.5, 0.5, -0.5, 0.5, -0.5, 0.5),
+         kind=1, b=(0.3, -0.2, 0.7)),
+    dict(id="cart_dipole", n=(20, 16, 12), coord="cart", dom=(1.0, 2.0, -0.5, 0.5, -0.5, 0.5),
+         kind=2, b=(0.0, 0.0, 0.0)),
+    dict(id="sph_dipole", n=(24, 20, 16), coord="sph",
+         dom=(1.0, 2.0, 0.25 * math.pi, 0.75 * math.pi, -0.25 * math.pi, 0.25 * math.pi),
+         kind=2, b=(0.0, 0.0, 0.0)),
+]
+
+
+@pytest.mark.parametrize("case", DEV_CASES, ids=[c["id"] for c in DEV_CASES])
+def test_device_background_matches_host_port(gop, case):
+    """set_background_field evaluated on the device (gop_set_background_device)
+    against the host port that equals the reference's arrays bit for bit:
+    every array agrees to 1e-13 of its largest value (the device's pow, sin
+    and cos and fused multiply-adds)."""
+    n, dom = case["n"], case["dom"]
+    xs = [gop.grid_uniform(n[a], dom[2 * a], dom[2 * a + 1]) for a in range(3)]
+    coord = gop.COORD_SPHERICAL if case["coord"] == "sph" else gop.COORD_CARTESIAN
+    host = gop.background_fields(n, xs, case["kind"], coord=coord, b=case["b"])
+    inst = gop.Instance(n, *xs, coord=coord, bc="eeeeee")
+    inst.set_background_device(case["kind"], b=case["b"])
+    dev = inst.get_background()
+    for k in ("b0", "lorentz", "b0_face", "b0_edge"):
+        scale = max(np.abs(host[k]).max(), 1e-300)
+        err = np.abs(dev[k] - host[k]).max() / scale
+        assert err <= 1e-13, (k, err)
+    inst.close()
+
+
+def test_device_background_steps_like_host_background(gop):
+    n = (24, 20, 16)
+    dom = (1.0, 2.0, -0.5, 0.5, -0.5, 0.5)
+    xs = [gop.grid_uniform(n[a], dom[2 * a], dom[2 * a + 1]) for a in range(3)]
+    out = []
+    for device in (False, True):
+        inst = gop.Instance(n, *xs, bc="eeeeee")
+        W0, B0 = inst.init_problem(gop.PROBLEM_BLAST, center=(1.5, 0.0, 0.0), b=(0.0, 0.0, 0.0))
+        if device:
+            inst.set_background_device(gop.BG_DIPOLE)
+        else:
+            inst.set_background(inst.background_fields(gop.BG_DIPOLE))
+        inst.upload(W0, B0)
+        inst.prepare()
+        inst.step(10)
+        out.append(inst.download(("gas", "face_b")))
+        inst.close()
+    errs = _errors(n, out[1], out[0]["gas"], out[0]["face_b"])
+    assert all(v <= 1e-12 for v in errs.values()), errs
