@@ -41,7 +41,8 @@ REF_BUDGET_S = 120  # seconds of timed steps the reference arm may spend
 GROUP_LAUNCHES = {"ab2": 1, "c2c": 3, "emf": 3, "flux": 3, "update": 1}
 # thread-block shapes the library's autotuner chooses from (gop_autotune)
 BLOCK_CANDIDATES = ["32x4x2", "32x8x1", "32x1x8", "32x2x4", "64x2x2", "64x4x1", "64x1x4",
-                    "128x2x1", "128x1x2", "32x4x1", "64x2x1", "256x1x1", "8x32x1", "8x4x8"]
+                    "128x2x1", "128x1x2", "32x4x1", "64x2x1", "256x1x1", "8x32x1", "8x4x8",
+                    "tma_sweep"]  # index 14 (GOP_TUNE_SWEEP): the tile-staged sweep kernel
 
 
 def peaks():
