@@ -28,11 +28,24 @@
 #include "gop_stage.cuh"
 
 #include <algorithm>
+#include <type_traits>
 #include <atomic>
 #include <cfloat>
 
 namespace gop {
 
+// Options of the mixed path's Cartesian update (0: FP32 as documented): run
+// the flux divergence, the Alfven/Boris correction or the CFL estimate in
+// FP64 instead
+#ifndef GOP_MX_DIV64
+#define GOP_MX_DIV64 0
+#endif
+#ifndef GOP_MX_ALF64
+#define GOP_MX_ALF64 0
+#endif
+#ifndef GOP_MX_CFL64
+#define GOP_MX_CFL64 0
+#endif
 
 // ------------------------------------------------------------------ utils
 
@@ -395,6 +408,11 @@ __device__ __forceinline__ double ct_face(const Params& P, const double* __restr
 template <typename R, bool BG, bool PSL>
 __device__ __forceinline__ void update_cart(const Params& P, const Work<R>& wk, Pos t,
                                             double& dtc, double& dbmax) {
+  // arithmetic of the stages the mixed path runs in FP32 (FP64 when their
+  // option is on, and always on the plain path)
+  using RD = typename std::conditional<sizeof(R) == 8 || GOP_MX_DIV64, double, R>::type;
+  using RA = typename std::conditional<sizeof(R) == 8 || GOP_MX_ALF64, double, R>::type;
+  using RC = typename std::conditional<sizeof(R) == 8 || GOP_MX_CFL64, double, R>::type;
   const int i = NGH + t.x, j = NGH + t.y, k = NGH + t.z;
   if (i >= NGH + P.n[0] || j >= NGH + P.n[1] || k >= NGH + P.n[2]) return;
   const size_t fs = P.fs;
@@ -464,9 +482,9 @@ __device__ __forceinline__ void update_cart(const Params& P, const Work<R>& wk, 
 #pragma unroll
   for (int a = 0; a < 3; a++) mt[a] = BG ? 0.5 * (mn[a] + mo[a]) + c0[a] : 0.5 * (mn[a] + mo[a]);
 
-  // flux divergence: 6 hydro and 3 stress components (R arithmetic when
-  // R = float; the reference's F_u A - F_l A over the volume otherwise)
-  R du[6], dm[3];
+  // flux divergence: 6 hydro and 3 stress components (FP32 arithmetic on
+  // the mixed path; the reference's F_u A - F_l A over the volume otherwise)
+  RD du[6], dm[3];
 #pragma unroll
   for (int d = 0; d < 3; d++) {
     const long long s = d == 0 ? 1LL : (d == 1 ? sj : sk);
@@ -474,11 +492,11 @@ __device__ __forceinline__ void update_cart(const Params& P, const Work<R>& wk, 
 #pragma unroll
     for (int m = 0; m < 9; m++) {
       if (m == PS && !PSL) continue;
-      R v;
-      if constexpr (sizeof(R) == 4) {
+      RD v;
+      if constexpr (sizeof(RD) == 4) {
         v = (Fd[s + m * fs] - Fd[m * fs]) * (R)il[d];
       } else {
-        v = (Fd[s + m * fs] * A[d] - Fd[m * fs] * A[d]) * ivol;
+        v = ((double)Fd[s + m * fs] * A[d] - (double)Fd[m * fs] * A[d]) * ivol;
       }
       if (m < 6) du[m] = d == 0 ? v : du[m] + v;
       else dm[m - 6] = d == 0 ? v : dm[m - 6] + v;
@@ -486,7 +504,7 @@ __device__ __forceinline__ void update_cart(const Params& P, const Work<R>& wk, 
   }
   if constexpr (BG) {  // + the Lorentz force of B0 (src/solver_solve.c:312-324)
 #pragma unroll
-    for (int a = 0; a < 3; a++) dm[a] += (R)P.bg[(size_t)(BG_LOR + a) * fs + x];
+    for (int a = 0; a < 3; a++) dm[a] += (RD)P.bg[(size_t)(BG_LOR + a) * fs + x];
   }
 
   // U^n from W^n, conservative update, cons->prim in FP64
@@ -521,23 +539,23 @@ __device__ __forceinline__ void update_cart(const Params& P, const Work<R>& wk, 
 
   // Alfven/Boris correction of the momentum (src/solver_solve.c:385-484)
   {
-    const R bsq = (R)(mt[0] * mt[0] + mt[1] * mt[1] + mt[2] * mt[2]);
-    const R alf = bsq / ((R)rho * (R)P.ca2);
-    const R perp = R(1) / (R(1) + alf);
-    const R rdt = (R)dt;
-    const R drho = -rdt * du[0];
-    const R dva = alf * drho;
-    R tv[3], wv[3];
+    const RA bsq = (RA)(mt[0] * mt[0] + mt[1] * mt[1] + mt[2] * mt[2]);
+    const RA alf = bsq / ((RA)rho * (RA)P.ca2);
+    const RA perp = RA(1) / (RA(1) + alf);
+    const RA rdt = (RA)dt;
+    const RA drho = -rdt * (RA)du[0];
+    const RA dva = alf * drho;
+    RA tv[3], wv[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-      wv[a] = (R)W[x + (1 + a) * fs];
-      tv[a] = alf * (-rdt * du[1 + a] - drho * wv[a]);
+      wv[a] = (RA)W[x + (1 + a) * fs];
+      tv[a] = alf * (-rdt * (RA)du[1 + a] - drho * wv[a]);
     }
-    R bdv = (R)mt[0] * tv[0] + (R)mt[1] * tv[1] + (R)mt[2] * tv[2];
-    bdv = bdv / (bsq + R(1e-10));
+    RA bdv = (RA)mt[0] * tv[0] + (RA)mt[1] * tv[1] + (RA)mt[2] * tv[2];
+    bdv = bdv / (bsq + RA(1e-10));
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-      const R inc = perp * ((-rdt * du[1 + a]) + (-rdt * dm[a]) + dva * wv[a] + (R)mt[a] * bdv);
+      const RA inc = perp * ((-rdt * (RA)du[1 + a]) + (-rdt * (RA)dm[a]) + dva * wv[a] + (RA)mt[a] * bdv);
       vv[a] = (U0[a] + (double)inc) * irho;
     }
   }
@@ -550,15 +568,15 @@ __device__ __forceinline__ void update_cart(const Params& P, const Work<R>& wk, 
 
   // CFL dt of the new state with magtot = mags^{n+1} (src/solver_func.c:255-298)
   {
-    const R r = (R)rho, u = (R)vv[0], v = (R)vv[1], w = (R)vv[2];
+    const RC r = (RC)rho, u = (RC)vv[0], v = (RC)vv[1], w = (RC)vv[2];
     const double t0 = mn[0] + c0[0], t1 = mn[1] + c0[1], t2 = mn[2] + c0[2];
-    const R bsq = BG ? (R)(t0 * t0 + t1 * t1 + t2 * t2) : (R)(mn[0] * mn[0] + mn[1] * mn[1] + mn[2] * mn[2]);
-    const R va = sqrt(bsq / r);
-    const R vae = va * (R)P.ca / sqrt(va * va + (R)P.ca2);
-    const R vf = sqrt(u * u + v * v + w * w);
-    const R vs = sqrt((R)P.gamma * (R)p / r);
-    const R vc = vf + sqrt(vs * vs + vae * vae);
-    dtc = (double)((R)P.cfl / (vc * (R)il[0] + vc * (R)il[1] + vc * (R)il[2]));
+    const RC bsq = BG ? (RC)(t0 * t0 + t1 * t1 + t2 * t2) : (RC)(mn[0] * mn[0] + mn[1] * mn[1] + mn[2] * mn[2]);
+    const RC va = sqrt(bsq / r);
+    const RC vae = va * (RC)P.ca / sqrt(va * va + (RC)P.ca2);
+    const RC vf = sqrt(u * u + v * v + w * w);
+    const RC vs = sqrt((RC)P.gamma * (RC)p / r);
+    const RC vc = vf + sqrt(vs * vs + vae * vae);
+    dtc = (double)((RC)P.cfl / (vc * (RC)il[0] + vc * (RC)il[1] + vc * (RC)il[2]));
   }
   if (!(dtc > 0.0) || !isfinite(p) || !isfinite(rho) || !isfinite(vv[0] + vv[1] + vv[2]))
     P.scal[S_FLAGS] = 1.0;
@@ -818,19 +836,20 @@ __device__ __forceinline__ void dt_body(const Params& P, Pos t, double& dtc, dou
     b3 += P.bg[(size_t)(BG_B0 + 2) * P.fs + c];
   }
   if constexpr (COORD == 0) {  // as update_cart
+    using RC = typename std::conditional<sizeof(R) == 8 || GOP_MX_CFL64, double, R>::type;
     const double dx[3] = {tb(P, 0, T_DX, i), tb(P, 1, T_DX, j), tb(P, 2, T_DX, k)};
     const double A[3] = {dx[1] * dx[2], dx[0] * dx[2], dx[0] * dx[1]};
     const double ivol = 1.0 / (dx[0] * dx[1] * dx[2]);
     const double il[3] = {A[0] * ivol, A[1] * ivol, A[2] * ivol};
-    const R r = (R)W[c], u = (R)W[c + P.fs], v = (R)W[c + 2 * P.fs], w = (R)W[c + 3 * P.fs];
-    const R p = (R)W[c + 4 * P.fs];
-    const R bsq = (R)(b1 * b1 + b2 * b2 + b3 * b3);
-    const R va = sqrt(bsq / r);
-    const R vae = va * (R)P.ca / sqrt(va * va + (R)P.ca2);
-    const R vf = sqrt(u * u + v * v + w * w);
-    const R vs = sqrt((R)P.gamma * p / r);
-    const R vc = vf + sqrt(vs * vs + vae * vae);
-    dtc = (double)((R)P.cfl / (vc * (R)il[0] + vc * (R)il[1] + vc * (R)il[2]));
+    const RC r = (RC)W[c], u = (RC)W[c + P.fs], v = (RC)W[c + 2 * P.fs], w = (RC)W[c + 3 * P.fs];
+    const RC p = (RC)W[c + 4 * P.fs];
+    const RC bsq = (RC)(b1 * b1 + b2 * b2 + b3 * b3);
+    const RC va = sqrt(bsq / r);
+    const RC vae = va * (RC)P.ca / sqrt(va * va + (RC)P.ca2);
+    const RC vf = sqrt(u * u + v * v + w * w);
+    const RC vs = sqrt((RC)P.gamma * p / r);
+    const RC vc = vf + sqrt(vs * vs + vae * vae);
+    dtc = (double)((RC)P.cfl / (vc * (RC)il[0] + vc * (RC)il[1] + vc * (RC)il[2]));
   } else if (P.ring && ring_band_row(P, j)) {  // as k_ring_dt
     dtc = cfl_cell<COORD>(P, i, j, k, W[c], W[c + P.fs], W[c + 2 * P.fs], W[c + 3 * P.fs],
                           W[c + 4 * P.fs], b1, b2, b3);
