@@ -77,6 +77,17 @@ def algorithmic_bytes(group, n, mixed=False, ps_live=False):
     return 0
 
 
+def fp64_flop_per_cell_update():
+    """FP64 FLOP of one plain cell-update (2 per DFMA, 1 per DADD / DMUL,
+    all step kernels) from the committed ncu summary, if any."""
+    import re
+    f = ROOT / "profiles" / "blast128_fp64_ops.md"
+    if not f.exists():
+        return None
+    m = re.search(r"flop_per_cell_update_fp64=([\d.]+)", f.read_text())
+    return float(m.group(1)) if m else None
+
+
 def ncu_traffic(group, mixed=False):
     """DRAM bytes per launch from the committed ncu summary, if any."""
     import re
@@ -398,6 +409,16 @@ def main():
     share = {g: round(v[0] / sum(x[0] for x in groups.values()), 4) for g, v in groups.items()}
     tr = ncu_traffic(dom, mixed=prec != 0)
 
+    # the secondary bound: FP64 arithmetic against the measured FP64 peak
+    fp64 = None
+    if prec == gop.PREC_FP64:
+        peak64 = gop.fp64_peak_tflops(stream.cuda_stream)
+        flop = fp64_flop_per_cell_update()
+        fp64 = {"peak_tflops": round(peak64, 2), "peak_kind": "measured (timed DFMA loop)",
+                "flop_per_cell_update": flop}
+        if flop:
+            ach = value / world * 1e6 * flop / 1e12
+            fp64.update({"achieved_tflops": round(ach, 3), "frac": round(ach / peak64, 4)})
     e2e = None
     if not args.no_e2e:
         e2e = measure_e2e(gop, torch, n, prec, args, max_all, barrier, world)
@@ -430,7 +451,8 @@ def main():
                      "algorithmic_bytes_per_launch": alg,
                      "avg_launch_ms": round(per_launch_s * 1e3, 4)},
         "step_roofline": {"bytes_per_cell_update": BYTES_PER_CELL_UPDATE,
-                          "achieved_gbs": round(step_gbs, 2), "frac": round(step_gbs / peak, 4)},
+                          "achieved_gbs": round(step_gbs, 2), "frac": round(step_gbs / peak, 4),
+                          "fp64": fp64},
         "kernel_share": share,
         "gpu_launches": int(launches),
         "final_time": st["time"], "divb_max": st["divb_max"],

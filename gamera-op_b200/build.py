@@ -19,6 +19,7 @@ SOURCES = [
     PKG / "csrc" / "gop_noalloc.cu",
     PKG / "csrc" / "gop_init.cu",
     PKG / "csrc" / "gop_bgdev.cu",
+    PKG / "csrc" / "gop_peak.cu",
     PKG / "csrc" / "gop_ring.cu",
     PKG / "host" / "gop_problems.c",
     PKG / "host" / "gop_background.c",

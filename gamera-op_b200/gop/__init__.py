@@ -105,6 +105,7 @@ def lib():
         L.gop_autotune.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
         L.gop_set_profiling.argtypes = [vp, C.c_int]
         L.gop_set_sweep.argtypes = [vp, C.c_int]
+        L.gop_measure_fp64_peak.argtypes = [_dp, vp]
         L.gop_get_profile.argtypes = [vp, _dp, C.POINTER(C.c_int64)]
         L.gop_batch_create.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(vp)]
         L.gop_batch_destroy.argtypes = [vp]
@@ -124,6 +125,13 @@ def _check(rc):
 
 def _ptr(a):
     return None if a is None else a.ctypes.data_as(_dp)
+
+
+def fp64_peak_tflops(stream_ptr=None) -> float:
+    """The device's measured FP64 peak (timed fused multiply-add loop)."""
+    v = C.c_double(0.0)
+    _check(lib().gop_measure_fp64_peak(C.byref(v), C.c_void_p(stream_ptr) if stream_ptr else None))
+    return v.value
 
 
 def kernel_launches() -> int:

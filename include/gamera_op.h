@@ -173,6 +173,12 @@ int gop_set_sweep(gop_instance *h, int on);
 int gop_set_profiling(gop_instance *h, int on);
 int gop_get_profile(gop_instance *h, double *ms, int64_t *count);
 
+/* Diagnostics: the device's FP64 arithmetic peak in TFLOP/s, measured by a
+ * timed loop of independent fused multiply-adds on `stream` (the
+ * denominator of the step's FP64 roofline).  No counterpart in the
+ * reference. */
+int gop_measure_fp64_peak(double *tflops, void *stream);
+
 /* Last error message of the calling thread ("" if none). */
 const char *gop_last_error(void);
 
