@@ -315,6 +315,9 @@ def main():
                          "ot: Orszag-Tang 256x256x4 to t=0.5; sphere: field loop on a "
                          "192x128x128 spherical shell for one crossing")
     ap.add_argument("--requests", type=int, default=160, help="served: stream length")
+    ap.add_argument("--rate", type=float, default=50.0,
+                    help="served: mean arrivals per second (50: the configured stream, about "
+                         "ten times one GPU's capacity; a few per second stays below it)")
     ap.add_argument("--members", type=int, default=96, help="batched: number of grids")
     ap.add_argument("--max-live", type=int, default=32, help="served: live request slots")
     args = ap.parse_args()
@@ -632,7 +635,7 @@ def bench_served(args, gop, torch, dist, rank, world, local, max_all, barrier):
     FP64 loop on the same requests; latency is time-to-solution."""
     from collections import Counter
     from gop import serve, workloads
-    jobs = workloads.served_stream(count=args.requests)
+    jobs = workloads.served_stream(count=args.requests, rate=args.rate)
     mine = serve.shard(jobs, rank, world)
     sample = lambda j: j.rid % 8 == 0
     # warm the kernels and the allocator on a small request
@@ -661,6 +664,8 @@ def bench_served(args, gop, torch, dist, rank, world, local, max_all, barrier):
         inst.close()
         return res
 
+    span = max(j.arrival for j in jobs) - min(j.arrival for j in jobs)
+    offered = sum(j.cells * j.steps for j in jobs) / max(span, 1e-9) / 1e6
     base_rep = serve.serial(mine, run_one)
     base = serve.combine(base_rep, dist)
     for o in base_rep.outcomes:
@@ -673,8 +678,8 @@ def bench_served(args, gop, torch, dist, rank, world, local, max_all, barrier):
         "n_gpus": world, "steps": sum(j.steps for j in jobs), "warmup": 1,
         "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64", "data": "synthetic",
-        "config": {"workload": f"served_poisson50_{len(jobs)}req_mixed", "requests": len(jobs),
-                   "rate_per_s": 50, "seed": 5150,
+        "config": {"workload": f"served_poisson{args.rate:g}_{len(jobs)}req_mixed",
+                   "requests": len(jobs), "rate_per_s": args.rate, "seed": 5150,
                    "grids": {"x".join(map(str, k)): v for k, v in sorted(Counter(j.n for j in jobs).items())},
                    "steps": "uniform [100, 1000]", "hbm_budget_gb": 150, "max_live": args.max_live,
                    "round_steps": 50, "host_workers": 4, "tolerance": 1e-5,
@@ -682,6 +687,10 @@ def bench_served(args, gop, torch, dist, rank, world, local, max_all, barrier):
                    "l2": "live states >> 126 MB L2"},
         "latency_s": {"p50": round(served["p50_s"], 3), "p99": round(served["p99_s"], 3),
                       "what": "time-to-solution: arrival to result on the host"},
+        "load": {"offered_mcell_updates_per_s": round(offered, 3),
+                 "utilisation": round(offered / served["mcell_updates_per_s"], 3),
+                 "what": "work of the stream over its arrival span, against the served "
+                         "throughput (above 1: requests queue for the GPU)"},
         "served": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in served.items()},
         "plain_fp64_one_at_a_time": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in base.items()},
         "speedup_vs_plain_fp64": round(served["mcell_updates_per_s"] / base["mcell_updates_per_s"], 3),
