@@ -48,6 +48,13 @@ def stale() -> bool:
     return any(p.stat().st_mtime > t for p in SOURCES + HEADERS)
 
 
+# per-source extra nvcc flags: the background field's quadratures and
+# stress differences keep the host port's operation order (no contraction
+# into fused multiply-adds), so they differ from it only by the device's
+# pow, sin and cos
+EXTRA = {"gop_bgdev.cu": ["-fmad=false"]}
+
+
 def build(force: bool = False, verbose: bool = False) -> Path:
     if not force and not stale():
         return LIB
@@ -57,7 +64,8 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     for src in SOURCES:
         obj = objdir / (src.stem + ".o")
         if src.suffix == ".cu":
-            cmd = [nvcc(), *NVCC_FLAGS, "-I", str(ROOT / "include"), "-c", str(src), "-o", str(obj)]
+            cmd = [nvcc(), *NVCC_FLAGS, *EXTRA.get(src.name, []), "-I", str(ROOT / "include"), "-c",
+                   str(src), "-o", str(obj)]
         else:
             cmd = ["gcc", "-std=gnu99", "-O2", "-fPIC", "-I", str(ROOT / "include"),
                    "-c", str(src), "-o", str(obj)]

@@ -229,11 +229,11 @@ __device__ __forceinline__ void load_fw(const double* __restrict__ fw, int tmax,
 // a1h = a1/2: the reference's |c1 p0 + c2 pm1| * 0.5 * a1 with the exact
 // factor 1/2 moved into a1.  Every other operation is the reference's, in
 // its order.
+// hi, lo: the larger and the smaller of lim[1], lim[2] (the clamp bounds)
 template <typename R>
 __device__ __forceinline__ void pdm_pair(const R v[8], const R lim[4], const FaceWeights<R>& W,
                                          R a1h, R a2, R s1, R q0l, R q0r, R L_ad0, R R_ad0,
-                                         R& L, R& Rr) {
-  const R hi = fmax(lim[1], lim[2]), lo = fmin(lim[1], lim[2]);
+                                         R hi, R lo, R& L, R& Rr) {
   {
     // left: cells f-4..f+2, limiter cells f-2 (im1), f-1 (i0), f (ip1)
     R fi = v[0] * W.wl[0];
@@ -292,7 +292,7 @@ __device__ __forceinline__ void recon_lr(const R v[8], const R lim[4], const Fac
   const R dm = lim[1] - lim[0], d1 = lim[2] - lim[1], dp = lim[3] - lim[2];
   const R s1 = sgn(d1);
   pdm_pair<R>(v, lim, W, a1h, a2, s1, fabs(sgn(dm) + s1), fabs(sgn(dp) + s1), fabs(dm),
-              fabs(dp), L, Rr);
+              fabs(dp), fmax(lim[1], lim[2]), fmin(lim[1], lim[2]), L, Rr);
 }
 
 // Weights of face f on axis AX for a warp whose lanes run along i: along
