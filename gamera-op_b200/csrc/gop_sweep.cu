@@ -73,9 +73,14 @@ constexpr int kSweepThreads = 32 * kWarps;
 #endif
 template <typename R>
 struct SweepCfg {
+  // the least number of slots; a kernel whose slots are small takes more
+  // (SlotRing below)
   static constexpr int STAGES = sizeof(R) == 8 ? GOP_SWEEP_STAGES_F64 : GOP_SWEEP_STAGES_F32;
   static constexpr int CTAS = sizeof(R) == 8 ? GOP_SWEEP_CTAS_F64 : GOP_SWEEP_CTAS_F32;
 };
+#ifndef GOP_SWEEP_MAX_STAGES
+#define GOP_SWEEP_MAX_STAGES 4
+#endif
 
 // a box of the slot: extents (x, y, z, fields) and elements, rounded up to
 // 32 so every box starts on a 128-byte boundary in FP32 and FP64
@@ -429,14 +434,26 @@ template <class Stage, typename R>
 __host__ __device__ constexpr int slot_bytes() {
   return Stage::ELEMS * (int)sizeof(R);
 }
+// Slots in a block's ring: as many as fit the SM's 228 KB of shared memory
+// at SweepCfg::CTAS blocks per SM (each block also reserves 1 KB), at least
+// SweepCfg::STAGES, at most GOP_SWEEP_MAX_STAGES.  The small slots of the
+// edge-EMF sweeps get 3-4: their tiles compute for less time than the
+// copies of the next take to land.
+template <class Stage, typename R>
+__host__ __device__ constexpr int ring_slots() {
+  constexpr int per_block = 228 * 1024 / SweepCfg<R>::CTAS - 1024 - 128 - 64;
+  constexpr int fit = per_block / slot_bytes<Stage, R>();
+  return fit < SweepCfg<R>::STAGES ? SweepCfg<R>::STAGES
+                                   : (fit > GOP_SWEEP_MAX_STAGES ? GOP_SWEEP_MAX_STAGES : fit);
+}
 template <class Stage, typename R>
 __host__ __device__ constexpr int sweep_smem() {
-  return SweepCfg<R>::STAGES * slot_bytes<Stage, R>() + 2 * SweepCfg<R>::STAGES * 8 + 128;
+  return ring_slots<Stage, R>() * slot_bytes<Stage, R>() + 2 * ring_slots<Stage, R>() * 8 + 128;
 }
 
 // Persistent sweep: lane 0 of warp 0 also feeds the ring.  It fills the
-// first STAGES slots, and after each tile waits until all 8 warps have
-// released that tile's slot, then issues the tile STAGES ahead into it; the
+// first S slots, and after each tile waits until all 8 warps have released
+// that tile's slot, then issues the tile S ahead into it; the
 // other warps meanwhile compute the next tile, whose copies were issued a
 // tile earlier.  Every wait is bounded; a block that gives up records the
 // failure in S_FLAGS (2) and drains its copies in flight before it exits.
@@ -445,7 +462,7 @@ __device__ __forceinline__ void sweep_run(const Params& P, const Work<R>& wk,
                                           const typename Stage::Maps& maps) {
   // stop flag, or an earlier pipeline wait that timed out: do nothing
   if (stopped(P) || P.scal[S_FLAGS] == 2.0) return;
-  constexpr int S = SweepCfg<R>::STAGES;
+  constexpr int S = ring_slots<Stage, R>();
   constexpr int SLOT = slot_bytes<Stage, R>();
   constexpr int TXB = Stage::TX * (int)sizeof(R);  // bytes the copies of one tile deliver
   static_assert(TXB <= SLOT, "slot holds its boxes");
