@@ -308,6 +308,8 @@ def main():
                     help="default workload: skip the mixed-precision run beside the FP64 one")
     ap.add_argument("--no-batched-sample", action="store_true",
                     help="default workload: skip the bounded batched sample")
+    ap.add_argument("--no-ot-sample", action="store_true",
+                    help="default workload: skip the Orszag-Tang run to t=0.5")
     ap.add_argument("--workload", default="blast256",
                     choices=["blast256", "batched", "served", "ot", "sphere"],
                     help="blast256: the single 256^3 grid (default); batched: 96 uneven "
@@ -433,6 +435,13 @@ def main():
     batched = None
     if prec == gop.PREC_FP64 and not args.no_batched_sample:
         batched = batched_sample(args, gop, torch, dist, rank, world, local, max_all, barrier)
+    ot = None
+    if prec == gop.PREC_FP64 and not args.no_ot_sample:
+        full = bench_ot(args, gop, torch, dist, rank, world, local, max_all, barrier)
+        ot = {k: full[k] for k in ("value", "ms_per_step", "steps", "plain_fp64",
+                                   "speedup_vs_plain_fp64", "accuracy_vs_fp64",
+                                   "fp64_sensitivity")}
+        ot["config"] = full["config"]
 
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
@@ -468,6 +477,8 @@ def main():
         line["mixed"] = mixed
     if batched:
         line["batched_sample"] = batched
+    if ot:
+        line["ot_to_t05"] = ot
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     if rank == 0:
