@@ -454,7 +454,8 @@ def main():
                    "parallelism": f"replicas x{world} (no data-path collective)",
                    "l2": "state 2.4 GB per replica >> 126 MB L2, no flush needed",
                    "precision": args.precision,
-                   "block_shapes": ({k: BLOCK_CANDIDATES[v] for k, v in tuned.items()} if tuned else "defaults")},
+                   "block_shapes": ({k: BLOCK_CANDIDATES[v] for k, v in tuned.items()} if tuned else "defaults"),
+                   "launch_order": inst.launch_order()},
         "latency_ms": {"p50": round(float(np.percentile(durs, 50)), 4),
                        "p99": round(float(np.percentile(durs, 99)), 4)},
         "roofline": {"bound": "hbm", "kernel": f"k_{dom}", "achieved": round(achieved, 2),

@@ -1073,6 +1073,50 @@ int gop_autotune(gop_instance* h, int reps, int* chosen) {
     if (chosen) chosen[slot] = best_c;
     drop_step_graph(h);  // the captured step has the old shapes
   }
+  // The order of the three flux launches and of the three EMF launches
+  // (independent launches: the order changes no result, only what L2 holds
+  // from one launch to the next): two whole steps timed per rotation of
+  // each, the whole state and its scalars restored after every trial.
+  for (int t = 0; t < NSCAL; t++) h->hscal[t] = saved_scal[t];
+  CK(cudaMemcpyAsync(P.Wbuf[1 - cur], hist, wbytes, cudaMemcpyDeviceToDevice, h->st));
+  CK(cudaMemcpyAsync(P.Bbuf[1 - cur], hist + 6 * P.fs, bbytes, cudaMemcpyDeviceToDevice, h->st));
+  {
+    double* full = nullptr;
+    const size_t sbytes = (size_t)P.fs * 18 * sizeof(double);
+    if (cudaMallocAsync((void**)&full, sbytes, h->st) == cudaSuccess) {
+      CK(cudaMemcpyAsync(full, h->state, sbytes, cudaMemcpyDeviceToDevice, h->st));
+      for (int which = 0; which < 2; which++) {
+        int* ord = which == 0 ? h->tune.flux_order : h->tune.emf_order;
+        const int base[3] = {ord[0], ord[1], ord[2]};
+        float best = 1e30f;
+        int best_r = 0;
+        for (int r = 0; r < 3; r++) {
+          for (int n = 0; n < 3; n++) ord[n] = base[(n + r) % 3];
+          launch_arm(P, 1e300, 3.0, h->st);
+          enqueue_one_step(h, h->st, Hook());  // warm-up
+          cudaEventRecord(a, h->st);
+          enqueue_one_step(h, h->st, Hook());
+          enqueue_one_step(h, h->st, Hook());
+          cudaEventRecord(b, h->st);
+          CK(cudaEventSynchronize(b));
+          float ms = 0.f;
+          cudaEventElapsedTime(&ms, a, b);
+          CK(cudaMemcpyAsync(h->state, full, sbytes, cudaMemcpyDeviceToDevice, h->st));
+          CK(cudaMemcpyAsync(h->scal, h->hscal, NSCAL * sizeof(double), cudaMemcpyHostToDevice, h->st));
+          if (ms < best) {
+            best = ms;
+            best_r = r;
+          }
+        }
+        for (int n = 0; n < 3; n++) ord[n] = base[(n + best_r) % 3];
+      }
+      CK(cudaStreamSynchronize(h->st));
+      cudaFreeAsync(full, h->st);
+      drop_step_graph(h);
+    } else {
+      cudaGetLastError();  // no room for the copy: the orders stay as they are
+    }
+  }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   CK(cudaMemcpyAsync(P.Wbuf[1 - cur], hist, wbytes, cudaMemcpyDeviceToDevice, h->st));
@@ -1083,6 +1127,15 @@ int gop_autotune(gop_instance* h, int reps, int* chosen) {
   cudaFreeAsync(hist, h->st);
   CK(cudaStreamSynchronize(h->st));
   CK(cudaGetLastError());
+  return GOP_OK;
+}
+
+int gop_get_launch_order(gop_instance* h, int* flux_order, int* emf_order) {
+  if (!h) return fail(GOP_EINVAL, "instance is NULL");
+  for (int d = 0; d < 3; d++) {
+    if (flux_order) flux_order[d] = h->tune.flux_order[d];
+    if (emf_order) emf_order[d] = h->tune.emf_order[d];
+  }
   return GOP_OK;
 }
 

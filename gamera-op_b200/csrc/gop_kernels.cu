@@ -1234,7 +1234,10 @@ Tune::Tune() {
   blk[K_C2C2] = blk[K_EMF2] = blk[K_FLUX2] = dim3(32, 1, 8);
   // the first edge sweep of edges along j covers only the 8 ghost layers of i
   blk[K_C2C1] = dim3(8, 32, 1);
-  for (int d = 0; d < 3; d++) flux_sweep[d] = emf_sweep[d] = true;
+  for (int d = 0; d < 3; d++) {
+    flux_sweep[d] = emf_sweep[d] = true;
+    flux_order[d] = emf_order[d] = d;
+  }
 }
 
 dim3 launch_space(const Params& P, int slot) {
@@ -1360,22 +1363,26 @@ void launch_step_body(const Params& P, int coord, const Work<R>& w, cudaStream_t
   launch_slot<R>(P, coord, w, K_AB2, tune.blk[K_AB2], st);
   hook(G_AB2, 0);
   // flux first: it also writes the edge velocities of the active range
+  // the three launches of a stage are independent (each axis writes its own
+  // fluxes, edge velocities or EMFs), so their order (Tune) changes no result
+  const int last_flux = tune.flux_order[2], last_emf = tune.emf_order[2];
   for (int stage : {2, 0, 1}) {
     const int g = stage == 0 ? G_C2C : (stage == 1 ? G_EMF : G_FLUX);
     hook(g, 1);
-    for (int d = 0; d < 3; d++) {
+    for (int n = 0; n < 3; n++) {
+      const int d = stage == 2 ? tune.flux_order[n] : (stage == 1 ? tune.emf_order[n] : n);
       const int slot = K_C2C0 + 3 * stage + d;
       const bool sweep = sw && ((stage == 2 && tune.flux_sweep[d]) || (stage == 1 && tune.emf_sweep[d]));
       // the launch after a persistent sweep grid waits for it to finish
       // instead of being placed early on SMs still configured for the
       // sweep's shared memory (and its short L1)
-      const bool pdl = !(stage == 0 && d == 0 && sw && tune.flux_sweep[2]) || GOP_PDL_AFTER_SWEEP;
+      const bool pdl = !(stage == 0 && n == 0 && sw && tune.flux_sweep[last_flux]) || GOP_PDL_AFTER_SWEEP;
       launch_slot<R>(P, coord, w, slot, tune.blk[slot], st, sweep ? sw : nullptr, pdl);
     }
     hook(g, 0);
   }
   hook(G_UPDATE, 1);
-  const bool after_emf_sweep = sw && tune.emf_sweep[2] && !GOP_PDL_AFTER_SWEEP;
+  const bool after_emf_sweep = sw && tune.emf_sweep[last_emf] && !GOP_PDL_AFTER_SWEEP;
   launch_pole_emf<R>(P, w, st);  // pole ring average only
   if (coord != 0) {  // curvilinear: the face fields in their own launch
     const dim3 blk = tune.blk[K_UPDATE];

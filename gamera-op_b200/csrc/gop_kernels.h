@@ -48,6 +48,9 @@ struct Tune {
   // sweeps apply
   bool flux_sweep[3];
   bool emf_sweep[3];
+  // order of the three (independent) launches of the flux and EMF stages
+  int flux_order[3];
+  int emf_order[3];
   Tune();
 };
 

@@ -105,6 +105,7 @@ def lib():
         L.gop_autotune.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
         L.gop_set_profiling.argtypes = [vp, C.c_int]
         L.gop_set_sweep.argtypes = [vp, C.c_int]
+        L.gop_get_launch_order.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.gop_measure_fp64_peak.argtypes = [_dp, vp]
         L.gop_get_profile.argtypes = [vp, _dp, C.POINTER(C.c_int64)]
         L.gop_batch_create.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(vp)]
@@ -313,6 +314,12 @@ class Instance:
         out = (C.c_int * len(self.TUNE_SLOTS))()
         _check(lib().gop_autotune(self._h, int(reps), out))
         return dict(zip(self.TUNE_SLOTS, list(out)))
+
+    def launch_order(self) -> dict:
+        """Axis order of the flux and EMF launches (chosen by autotune)."""
+        f, e = (C.c_int * 3)(), (C.c_int * 3)()
+        _check(lib().gop_get_launch_order(self._h, f, e))
+        return {"flux": list(f), "emf": list(e)}
 
     def set_sweep(self, on: bool):
         """Face fluxes by the tile-staged sweep kernels (default) or the

@@ -150,11 +150,17 @@ int gop_get_stats(gop_instance *h, gop_stats *out);
 /* Autotuner: times candidate thread-block shapes for each of the 11
  * tunable launches of a step on the instance's current state (after
  * gop_prepare; the state is not advanced) and keeps the fastest for the
- * following steps.  reps: timed launches per candidate (0 = 3); chosen
- * (optional, 11 ints) receives the picked candidate index per launch. */
+ * following steps; then the order of the three flux launches and of the
+ * three edge-EMF launches (each order a rotation of the axes; the launches
+ * are independent, so no result changes), timing two whole steps per
+ * rotation with the state restored after each.  reps: timed launches per
+ * candidate (0 = 3); chosen (optional, 11 ints) receives the picked
+ * candidate index per launch. */
 #define GOP_NTUNE 11
 #define GOP_TUNE_SWEEP 14 /* chosen[] value of a flux or EMF launch: the tile-staged sweep kernel */
 int gop_autotune(gop_instance *h, int reps, int *chosen);
+/* The launch orders the autotuner picked (axes, 3 ints each; may be NULL). */
+int gop_get_launch_order(gop_instance *h, int *flux_order, int *emf_order);
 
 /* Kernel choice for the face fluxes and edge EMFs: on (the default) runs
  * the tile-staged sweep kernels (shared-memory tiles filled by the Tensor

@@ -123,3 +123,35 @@ def test_autotune_may_pick_the_sweep(gop):
     inst.step(3)
     assert inst.stats()["flags"] == 0
     inst.close()
+
+
+def test_autotuned_launch_order_changes_no_result(gop):
+    """The autotuner also picks the order of the three flux launches and of
+    the three EMF launches (rotations of the axes) by timing whole steps, and
+    restores the state after each trial: a tuned instance steps to the same
+    state as an untuned one."""
+    n = (48, 40, 32)
+    xs = _grid(gop, n, (-0.5, 0.5) * 3)
+    probe = gop.Instance(n, *xs)
+    W0, B0 = probe.init_problem(gop.PROBLEM_BLAST, b=(0.4, 0.5, 0.3))
+    probe.close()
+    out = []
+    for tune in (True, False):
+        inst = gop.Instance(n, *xs)
+        inst.upload(W0, B0)
+        inst.prepare()
+        if tune:
+            inst.autotune(reps=1)
+            order = inst.launch_order()
+            rot = [[0, 1, 2], [1, 2, 0], [2, 0, 1]]
+            assert order["flux"] in rot and order["emf"] in rot, order
+        else:
+            assert inst.launch_order() == {"flux": [0, 1, 2], "emf": [0, 1, 2]}
+        inst.step(8)
+        out.append((inst.download(("gas", "face_b")), inst.stats()))
+        inst.close()
+    (a, sa), (b, sb) = out
+    errs = _diff(n, a, b)
+    assert all(v <= TOL for v in errs.values()), errs
+    assert sa["steps"] == sb["steps"] == 8
+    assert math.isclose(sa["time"], sb["time"], rel_tol=1e-13)
