@@ -1078,6 +1078,7 @@ int gop_autotune(gop_instance* h, int reps, int* chosen) {
   // from one launch to the next): two whole steps timed per rotation of
   // each, the whole state and its scalars restored after every trial.
   for (int t = 0; t < NSCAL; t++) h->hscal[t] = saved_scal[t];
+  CK(cudaMemcpyAsync(h->scal, h->hscal, NSCAL * sizeof(double), cudaMemcpyHostToDevice, h->st));
   CK(cudaMemcpyAsync(P.Wbuf[1 - cur], hist, wbytes, cudaMemcpyDeviceToDevice, h->st));
   CK(cudaMemcpyAsync(P.Bbuf[1 - cur], hist + 6 * P.fs, bbytes, cudaMemcpyDeviceToDevice, h->st));
   {
