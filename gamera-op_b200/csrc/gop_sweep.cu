@@ -64,6 +64,13 @@ constexpr int kSweepThreads = 32 * kWarps;
 #ifndef GOP_SWEEP_CTAS_F32
 #define GOP_SWEEP_CTAS_F32 3
 #endif
+// blocks per SM of the edge-EMF sweeps (smaller slots than the flux sweeps)
+#ifndef GOP_SWEEP_EMF_CTAS_F64
+#define GOP_SWEEP_EMF_CTAS_F64 GOP_SWEEP_CTAS_F64
+#endif
+#ifndef GOP_SWEEP_EMF_CTAS_F32
+#define GOP_SWEEP_EMF_CTAS_F32 GOP_SWEEP_CTAS_F32
+#endif
 // 1: the sweeps go out with programmatic dependent launch like the other
 // step kernels.  Off: a sweep grid placed early onto SMs that still run the
 // previous kernel (persistent blocks, no room to spare) measured 2-20 %
@@ -71,12 +78,13 @@ constexpr int kSweepThreads = 32 * kWarps;
 #ifndef GOP_SWEEP_PDL
 #define GOP_SWEEP_PDL 0
 #endif
-template <typename R>
+template <typename R, bool EMF>
 struct SweepCfg {
   // the least number of slots; a kernel whose slots are small takes more
-  // (SlotRing below)
+  // (ring_slots below)
   static constexpr int STAGES = sizeof(R) == 8 ? GOP_SWEEP_STAGES_F64 : GOP_SWEEP_STAGES_F32;
-  static constexpr int CTAS = sizeof(R) == 8 ? GOP_SWEEP_CTAS_F64 : GOP_SWEEP_CTAS_F32;
+  static constexpr int CTAS = EMF ? (sizeof(R) == 8 ? GOP_SWEEP_EMF_CTAS_F64 : GOP_SWEEP_EMF_CTAS_F32)
+                                  : (sizeof(R) == 8 ? GOP_SWEEP_CTAS_F64 : GOP_SWEEP_CTAS_F32);
 };
 #ifndef GOP_SWEEP_MAX_STAGES
 #define GOP_SWEEP_MAX_STAGES 4
@@ -164,6 +172,7 @@ __device__ __forceinline__ TileAt flux_at(const int nt[3], int t) {
 
 template <typename R, int D, bool BG>
 struct FluxStage {
+  static constexpr bool EMF = false;
   using F = FluxTile<D>;
   using Maps = FluxMaps;
   static constexpr int ELEMS = F::ELEMS;
@@ -300,6 +309,7 @@ __device__ __forceinline__ TileAt emf_at(const int nt[3], int t) {
 
 template <typename R, int D, bool BG>
 struct EmfStage {
+  static constexpr bool EMF = true;
   using E = EmfTile<D>;
   using Maps = EmfMaps;
   static constexpr int ELEMS = E::ELEMS;
@@ -441,9 +451,10 @@ __host__ __device__ constexpr int slot_bytes() {
 // copies of the next take to land.
 template <class Stage, typename R>
 __host__ __device__ constexpr int ring_slots() {
-  constexpr int per_block = 228 * 1024 / SweepCfg<R>::CTAS - 1024 - 128 - 64;
+  using Cfg = SweepCfg<R, Stage::EMF>;
+  constexpr int per_block = 228 * 1024 / Cfg::CTAS - 1024 - 128 - 64;
   constexpr int fit = per_block / slot_bytes<Stage, R>();
-  return fit < SweepCfg<R>::STAGES ? SweepCfg<R>::STAGES
+  return fit < Cfg::STAGES ? Cfg::STAGES
                                    : (fit > GOP_SWEEP_MAX_STAGES ? GOP_SWEEP_MAX_STAGES : fit);
 }
 template <class Stage, typename R>
@@ -525,14 +536,14 @@ __device__ __forceinline__ void sweep_run(const Params& P, const Work<R>& wk,
 }
 
 template <typename R, int D, bool BG>
-__global__ void __launch_bounds__(kSweepThreads, SweepCfg<R>::CTAS)
+__global__ void __launch_bounds__(kSweepThreads, (SweepCfg<R, false>::CTAS))
     k_flux_sweep(Params P, Work<R> wk, const __grid_constant__ FluxMaps maps) {
   pdl_enter();
   sweep_run<FluxStage<R, D, BG>, R>(P, wk, maps);
 }
 
 template <typename R, int D, bool BG>
-__global__ void __launch_bounds__(kSweepThreads, SweepCfg<R>::CTAS)
+__global__ void __launch_bounds__(kSweepThreads, (SweepCfg<R, true>::CTAS))
     k_emf_sweep(Params P, Work<R> wk, const __grid_constant__ EmfMaps maps) {
   pdl_enter();
   sweep_run<EmfStage<R, D, BG>, R>(P, wk, maps);
@@ -540,8 +551,8 @@ __global__ void __launch_bounds__(kSweepThreads, SweepCfg<R>::CTAS)
 
 template <typename R, int D>
 constexpr bool smem_fits() {
-  return (size_t)sweep_smem<FluxStage<R, D, false>, R>() * SweepCfg<R>::CTAS <= 228 * 1024 &&
-         (size_t)sweep_smem<EmfStage<R, D, false>, R>() * SweepCfg<R>::CTAS <= 228 * 1024;
+  return (size_t)sweep_smem<FluxStage<R, D, false>, R>() * SweepCfg<R, false>::CTAS <= 228 * 1024 &&
+         (size_t)sweep_smem<EmfStage<R, D, false>, R>() * SweepCfg<R, true>::CTAS <= 228 * 1024;
 }
 static_assert(smem_fits<double, 0>() && smem_fits<double, 1>() && smem_fits<double, 2>(),
               "FP64 sweep blocks per SM");
@@ -717,7 +728,7 @@ template <class Stage, typename R, class Maps, class K>
 static void launch_persistent(K kern, const SweepSet* sw, const Params& P, const Work<R>& w,
                               const Maps& m, cudaStream_t st) {
   const int ntiles = m.nt[0] * m.nt[1] * m.nt[2];
-  const int grid = std::max(1, std::min(ntiles, sw->sms * SweepCfg<R>::CTAS));
+  const int grid = std::max(1, std::min(ntiles, sw->sms * SweepCfg<R, Stage::EMF>::CTAS));
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   at[0].val.programmaticStreamSerializationAllowed = 1;
