@@ -208,27 +208,50 @@ __device__ __forceinline__ void ab2_body(const Params& P, const Work<R>& w, Pos 
   const long long x = lin(P, i, j, k);
   const size_t fs = P.fs;
   const bool ci = i < P.N[0] - 1, cj = j < P.N[1] - 1, ck = k < P.N[2] - 1;
-  if (ci && cj && ck) {
+  // all loads first, then the stores: with FP64 work arrays the compiler
+  // cannot tell them from the state, and a store between two loads would
+  // keep the second from being issued ahead
+  constexpr int NW = PSL ? 6 : 5;
+  const bool inner = ci && cj && ck;
+  double v[NW], vo[NW], ms[3], mo[3], b[3], bo[3];
+  bool ok[3];
+  if (inner) {
 #pragma unroll
-    for (int m = 0; m < (PSL ? 6 : 5); m++) {
-      const double v = W[x + m * fs], vo = Wo[x + m * fs];
-      w.Wh[x + m * fs] = (R)(v + c * (v - vo));
-      if constexpr (sizeof(R) == 4) w.Wl[x + m * fs] = (R)v;
+    for (int m = 0; m < NW; m++) {
+      v[m] = W[x + m * fs];
+      vo[m] = Wo[x + m * fs];
     }
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-      const double ms = mags_at(P, B, a, i, j, k), mo = mags_at(P, Bo, a, i, j, k);
-      w.Ms[x + a * fs] = (R)ms;
-      w.Msh[x + a * fs] = (R)(ms + c * (ms - mo));
+      ms[a] = mags_at(P, B, a, i, j, k);
+      mo[a] = mags_at(P, Bo, a, i, j, k);
     }
   }
 #pragma unroll
   for (int a = 0; a < 3; a++) {
-    const bool ok = (a == 0 || ci) && (a == 1 || cj) && (a == 2 || ck);
-    if (ok) {
-      const double b = B[x + a * fs], bo = Bo[x + a * fs];
-      w.Bh[x + a * fs] = (R)(b + c * (b - bo));
-      if constexpr (sizeof(R) == 4) w.Bl[x + a * fs] = (R)b;
+    ok[a] = (a == 0 || ci) && (a == 1 || cj) && (a == 2 || ck);
+    if (ok[a]) {
+      b[a] = B[x + a * fs];
+      bo[a] = Bo[x + a * fs];
+    }
+  }
+  if (inner) {
+#pragma unroll
+    for (int m = 0; m < NW; m++) {
+      w.Wh[x + m * fs] = (R)(v[m] + c * (v[m] - vo[m]));
+      if constexpr (sizeof(R) == 4) w.Wl[x + m * fs] = (R)v[m];
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      w.Ms[x + a * fs] = (R)ms[a];
+      w.Msh[x + a * fs] = (R)(ms[a] + c * (ms[a] - mo[a]));
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    if (ok[a]) {
+      w.Bh[x + a * fs] = (R)(b[a] + c * (b[a] - bo[a]));
+      if constexpr (sizeof(R) == 4) w.Bl[x + a * fs] = (R)b[a];
     }
   }
 }
@@ -450,12 +473,19 @@ __device__ __forceinline__ void update_cart(const Params& P, const Work<R>& wk, 
   mo[0] = B[x] * tb(P, 0, T_MA, i) + B[x + 1] * tb(P, 0, T_MB, i);
   mo[1] = B[x + fs] * tb(P, 1, T_MA, j) + B[x + sj + fs] * tb(P, 1, T_MB, j);
   mo[2] = B[x + 2 * fs] * tb(P, 2, T_MA, k) + B[x + sk + 2 * fs] * tb(P, 2, T_MB, k);
-  Bn[x] = bl[0];
-  Bn[x + fs] = bl[1];
-  Bn[x + 2 * fs] = bl[2];
-  if (i == NGH + P.n[0] - 1) Bn[x + 1] = bu[0];
-  if (j == NGH + P.n[1] - 1) Bn[x + sj + fs] = bu[1];
-  if (k == NGH + P.n[2] - 1) Bn[x + sk + 2 * fs] = bu[2];
+  auto store_b = [&]() {
+    Bn[x] = bl[0];
+    Bn[x + fs] = bl[1];
+    Bn[x + 2 * fs] = bl[2];
+    if (i == NGH + P.n[0] - 1) Bn[x + 1] = bu[0];
+    if (j == NGH + P.n[1] - 1) Bn[x + sj + fs] = bu[1];
+    if (k == NGH + P.n[2] - 1) Bn[x + sk + 2 * fs] = bu[2];
+  };
+  // FP64: the face field is stored after the last load (the next state's
+  // buffers could alias the FP64 work arrays as far as the compiler knows,
+  // and a store ahead of the flux loads would hold them back); FP32 work
+  // arrays cannot alias it, and storing it here frees registers
+  if constexpr (sizeof(R) == 4) store_b();
   if constexpr (BG) {  // div of B + B0 (face-normal B0, src/solver_func.c:324-343)
     const double* f0 = P.bg + (size_t)BG_FACE * fs + x;
     const double* f1 = P.bg + (size_t)(BG_FACE + 4) * fs + x;
@@ -559,6 +589,7 @@ __device__ __forceinline__ void update_cart(const Params& P, const Work<R>& wk, 
       vv[a] = (U0[a] + (double)inc) * irho;
     }
   }
+  if constexpr (sizeof(R) == 8) store_b();
   Wn[x] = rho;
   Wn[x + fs] = vv[0];
   Wn[x + 2 * fs] = vv[1];
