@@ -1268,6 +1268,88 @@ static int batch_build(gop_batch* b) {
   return GOP_OK;
 }
 
+// The sweep kernels were picked per class with each grid stepping alone.
+// In the batch the members' launches run side by side on parallel branches,
+// and a persistent sweep grid (sized for the whole GPU) then shares the SMs
+// with the other branches' kernels.  Times replays of the batch step with
+// the per-class picks and with every member on the per-point kernels, the
+// member states and scalars restored after each trial, and keeps the
+// faster.  Without device memory for the copies of the states the picks
+// stay as they are.
+static int batch_pick_sweeps(gop_batch* b) {
+  bool any = false;
+  for (gop_instance* h : b->m)
+    for (int d = 0; d < 3; d++) any = any || h->tune.flux_sweep[d] || h->tune.emf_sweep[d];
+  if (!any || !b->graph) return GOP_OK;
+  const size_t nm = b->m.size();
+  std::vector<double*> saved(nm, nullptr);
+  std::vector<double> scal(nm * NSCAL);
+  bool ok = true;
+  for (size_t i = 0; i < nm && ok; i++) {
+    gop_instance* h = b->m[i];
+    const size_t bytes = (size_t)h->P.fs * 18 * sizeof(double);
+    ok = cudaMallocAsync((void**)&saved[i], bytes, b->st) == cudaSuccess &&
+         cudaMemcpyAsync(saved[i], h->state, bytes, cudaMemcpyDeviceToDevice, b->st) == cudaSuccess &&
+         cudaMemcpyAsync(&scal[i * NSCAL], h->scal, NSCAL * sizeof(double), cudaMemcpyDeviceToHost,
+                         b->st) == cudaSuccess;
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  ok = ok && cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess &&
+       cudaStreamSynchronize(b->st) == cudaSuccess;
+  int rc = GOP_OK;
+  // two timed replays after a warm-up one, then every member put back
+  auto trial = [&](float* ms) {
+    for (gop_instance* h : b->m) launch_arm(h->P, 1e300, 3.0, b->st);
+    cudaGraphLaunch(b->graph, b->st);
+    cudaEventRecord(e0, b->st);
+    cudaGraphLaunch(b->graph, b->st);
+    cudaGraphLaunch(b->graph, b->st);
+    cudaEventRecord(e1, b->st);
+    count_launches(3 * b->nodes);
+    cudaError_t e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(ms, e0, e1);
+    for (size_t i = 0; i < nm && e == cudaSuccess; i++) {
+      gop_instance* h = b->m[i];
+      e = cudaMemcpyAsync(h->state, saved[i], (size_t)h->P.fs * 18 * sizeof(double),
+                          cudaMemcpyDeviceToDevice, b->st);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(h->scal, &scal[i * NSCAL], NSCAL * sizeof(double),
+                            cudaMemcpyHostToDevice, b->st);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->st);
+    if (e != cudaSuccess) rc = fail(GOP_ECUDA, "batch sweep trial failed: %s", cudaGetErrorString(e));
+  };
+  if (ok) {
+    float t_pick = 0.f, t_off = 0.f;
+    trial(&t_pick);
+    std::vector<Tune> pick(nm);
+    for (size_t i = 0; i < nm; i++) pick[i] = b->m[i]->tune;
+    for (gop_instance* h : b->m) {
+      for (int d = 0; d < 3; d++) h->tune.flux_sweep[d] = h->tune.emf_sweep[d] = false;
+      drop_step_graph(h);
+    }
+    if (rc == GOP_OK) rc = batch_build(b);
+    if (rc == GOP_OK) trial(&t_off);
+    if (rc != GOP_OK || t_pick <= t_off) {
+      for (size_t i = 0; i < nm; i++) {
+        b->m[i]->tune = pick[i];
+        drop_step_graph(b->m[i]);
+      }
+      const int rc2 = batch_build(b);
+      if (rc == GOP_OK) rc = rc2;
+    }
+  } else {
+    cudaGetLastError();  // no room for the copies: the picks stay
+  }
+  cudaStreamSynchronize(b->st);
+  for (double* p : saved)
+    if (p) cudaFreeAsync(p, b->st);
+  cudaStreamSynchronize(b->st);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  return rc;
+}
+
 extern "C" {
 
 int gop_batch_create(gop_instance* const* members, int count, gop_batch** out) {
@@ -1361,7 +1443,8 @@ int gop_batch_autotune(gop_batch* b, int reps, int* chosen) {
       for (int t = 0; t < NTUNE; t++) chosen[t] = pick[t];
     }
   }
-  return batch_build(b);
+  const int rc = batch_build(b);
+  return rc ? rc : batch_pick_sweeps(b);
 }
 
 int gop_batch_launch(gop_batch* b, const int* steps) {

@@ -349,10 +349,15 @@ int gop_batch_wait(gop_batch *b);
 int gop_batch_set_stream(gop_batch *b, void *stream);
 /* Chooses thread-block shapes for the members: gop_autotune on the first
  * member of each class of equal grid shape, geometry and precision, copied
- * to the rest of the class, then captures the batch graph again;
- * chosen[GOP_NTUNE] (may be NULL) receives the candidate indices of the
- * class with the most cells.  The state and scalars of every member are
- * left as they were. */
+ * to the rest of the class, then captures the batch graph again; then
+ * times replays of the batch step with those picks and with every member
+ * on the per-point flux and EMF kernels (the tile-staged sweeps, picked
+ * with each grid alone, share the SMs with the other members' kernels in
+ * a batch) and keeps the faster (skipped without device memory for a copy
+ * of every member's state).  chosen[GOP_NTUNE] (may be NULL) receives the
+ * candidate indices of the class with the most cells, as gop_autotune
+ * picked them.  The state and scalars of every member are left as they
+ * were. */
 int gop_batch_autotune(gop_batch *b, int reps, int *chosen);
 
 #ifdef __cplusplus

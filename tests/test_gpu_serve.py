@@ -79,7 +79,8 @@ def test_batch_autotune_keeps_state_and_results(gop):
     members = [workloads.build(j) for j in jobs]
     b = gop.Batch(members)
     chosen = b.autotune(reps=1)
-    assert len(chosen) == 11 and all(0 <= v < 14 for v in chosen.values())
+    # candidate 14 (GOP_TUNE_SWEEP) is the tile-staged sweep of a flux or EMF launch
+    assert len(chosen) == 11 and all(0 <= v <= 14 for v in chosen.values())
     b.step([j.steps for j in jobs])
     for a, m in zip(alone, members):
         d = m.download(("gas", "face_b"))
@@ -92,3 +93,37 @@ def test_batch_autotune_keeps_state_and_results(gop):
         d = m.download(("gas", "face_b"))
         assert np.array_equal(d["gas"], d0["gas"])
         assert np.array_equal(d["face_b"], d0["face_b"])
+
+
+def test_batch_autotune_with_sweep_sized_members_keeps_state_and_results(gop):
+    """Members large enough for the sweep kernels: the batch autotune also
+    times the batch step with and without them (restoring every member
+    after each trial), and the batch still ends bit-identical to each
+    member stepped alone."""
+    shapes = [(96, 96, 96), (64, 64, 64), (96, 64, 32)]
+    alone = []
+    for n in shapes:
+        a = gop.make(gop.PROBLEM_BLAST, n, b=(0.4, 0.5, 0.3))
+        a.prepare()
+        a.step(6)
+        alone.append(a.download(("gas", "face_b")))
+        a.close()
+    members = [gop.make(gop.PROBLEM_BLAST, n, b=(0.4, 0.5, 0.3)) for n in shapes]
+    for m in members:
+        m.prepare()
+    b = gop.Batch(members)
+    before = [m.download(("gas", "face_b")) for m in members]
+    b.autotune(reps=1)
+    for m, d0 in zip(members, before):
+        d = m.download(("gas", "face_b"))
+        assert np.array_equal(d["gas"], d0["gas"])
+        assert np.array_equal(d["face_b"], d0["face_b"])
+        assert m.stats()["steps"] == 0
+    b.step([6] * len(members))
+    for a, m in zip(alone, members):
+        d = m.download(("gas", "face_b"))
+        assert np.array_equal(d["gas"], a["gas"])
+        assert np.array_equal(d["face_b"], a["face_b"])
+    b.close()
+    for m in members:
+        m.close()
