@@ -46,19 +46,9 @@ namespace gop {
 #ifndef GOP_MX_CFL64
 #define GOP_MX_CFL64 0
 #endif
-// 1: the Cartesian update asks L2 for its face fluxes and state at entry,
-// ahead of the constrained-transport arithmetic and stores
-#ifndef GOP_UPD_PREFETCH
-#define GOP_UPD_PREFETCH 0
-#endif
 
 // ------------------------------------------------------------------ utils
 
-
-// a hint to bring the line holding p into L2 (generic address, no result)
-__device__ __forceinline__ void prefetch_l2(const void* p) {
-  asm volatile("prefetch.L2 [%0];" ::"l"(p));
-}
 
 __device__ __forceinline__ void atomic_min_pos(double* slot, double v) {
   // positive doubles order like their bit patterns
@@ -456,22 +446,6 @@ __device__ __forceinline__ void update_cart(const Params& P, const Work<R>& wk, 
   double* __restrict__ Wn = P.Wbuf[1 - cb];
   double* __restrict__ Bn = P.Bbuf[1 - cb];
   const long long x = lin(P, i, j, k), sj = P.sj, sk = P.sk;
-#if GOP_UPD_PREFETCH
-  {
-    const R* F = wk.F + x;
-#pragma unroll
-    for (int m = 0; m < 9; m++) {
-      if (m == PS && !PSL) continue;
-      prefetch_l2(F + (size_t)m * fs);
-      prefetch_l2(F + (size_t)(9 + m) * fs);
-      prefetch_l2(F + (size_t)(9 + m) * fs + sj);
-      prefetch_l2(F + (size_t)(18 + m) * fs);
-      prefetch_l2(F + (size_t)(18 + m) * fs + sk);
-    }
-#pragma unroll
-    for (int m = 0; m < 5; m++) prefetch_l2(W + x + (size_t)m * fs);
-  }
-#endif
   const double dx[3] = {tb(P, 0, T_DX, i), tb(P, 1, T_DX, j), tb(P, 2, T_DX, k)};
   const double A[3] = {dx[1] * dx[2], dx[0] * dx[2], dx[0] * dx[1]};
   const double ivol = 1.0 / (dx[0] * dx[1] * dx[2]);
