@@ -155,6 +155,17 @@ def host_cores():
     return os.cpu_count() or 1
 
 
+def cpu_model():
+    """The host CPU's model name, as /proc/cpuinfo gives it."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def rank_dims(cores, n):
     """The reference's process grid for about `cores` ranks: the largest
     power of two not above it, split over the axes as evenly as the grid
@@ -210,6 +221,7 @@ def cpu_baseline(n=(128, 128, 128), steps=4):
             cells = n[0] * n[1] * n[2]
             v = cells * r.wall_steps / r.wall_seconds / 1e6
             return {"value": round(v, 4), "unit": UNIT, "cores": ranks, "kind": "reference",
+                    "cpu": cpu_model(),
                     "sample": f"reference Release build, {ranks} ranks x 1 thread "
                               f"(process grid {dims[0]}x{dims[1]}x{dims[2]}), blast {n[0]}^3, "
                               f"{r.wall_steps} timed steps after 1"}
@@ -273,6 +285,7 @@ def run_reference(args, rank):
            "grid": list(full),
            "problem": "blast p_in=10 p_out=0.1 r=0.1 B=(1/sqrt2,1/sqrt2,0) gamma=5/3 CFL=0.3",
            "ranks": ranks, "process_grid": list(dims), "threads_per_rank": 1,
+           "cpu": cpu_model(), "host_physical_cores": cores,
            "mode": "mpirun -n N, OMP_NUM_THREADS=1 (the reference README's mode), "
                    "through the fork-based MPI stand-in"}
     if n != full:
