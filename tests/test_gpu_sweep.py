@@ -1,15 +1,17 @@
-"""The tile-staged flux sweeps (gop_sweep.cu) against the per-face flux
-kernels they replace.
+"""The tile-staged flux and edge-EMF sweeps (gop_sweep.cu) against the
+per-face and per-edge kernels they replace.
 
 Both compute every face with the same arithmetic in the same order, so the
 same state stepped with either must come out the same: the tests allow
 1e-13 relative L1 per variable (round-off from a different contraction of
 a multiply-add by the compiler) and report the largest difference.  The
 cases cover what changes the sweeps' tiles: partial tiles on every axis
-(ragged sizes), thin axes (4 cells), a spherical grid with its per-face
-weight tables, boundary fills, a background field and the FP32 stages of
-the mixed path.  Parity of the default path with the reference itself is
-in test_gpu_parity.py, which now runs the sweeps.
+(ragged sizes), i rows whose upper boundary face is computed by the last
+tile's row-end pass (ni a multiple of 32), thin axes (4 cells), a
+spherical grid with its per-face weight tables, boundary fills, a
+background field and the FP32 stages of the mixed path.  Parity of the
+default path with the reference itself is in test_gpu_parity.py, which
+runs the sweeps.
 """
 import math
 
@@ -73,6 +75,13 @@ CASES = [
     dict(id="sphere_mixed", n=(67, 35, 19),
          dom=(1.0, 2.0, 0.25 * math.pi, 0.75 * math.pi, -0.25 * math.pi, 0.25 * math.pi),
          coord=2, bc="eeeeee", kind="loop_sph", prec=1, steps=12),
+    # ni a multiple of 32: the i rows' upper boundary faces come with the
+    # last tile of each row (the row-end pass of the i-face sweeps)
+    dict(id="blast_64x48x40_mixed", n=(64, 48, 40), dom=(-0.5, 0.5) * 3, coord=0, bc="pppppp",
+         kind="blast", prec=1, steps=12),
+    dict(id="sphere_96x35x19", n=(96, 35, 19),
+         dom=(1.0, 2.0, 0.25 * math.pi, 0.75 * math.pi, -0.25 * math.pi, 0.25 * math.pi),
+         coord=2, bc="eeeeee", kind="loop_sph", prec=0, steps=12),
 ]
 
 
