@@ -99,43 +99,37 @@ struct Box {
 };
 constexpr Box kRec8{FW, 8, 1, 1};    // 8 packed face records
 constexpr Box kRec1{FW, 1, 1, 1};    // 1 packed face record
-// tap-major weights (T_WL0..T_CR2) of the 32 faces of a warp row and of the
-// face after them (a sweep whose lanes run along the faces of its axis)
-constexpr Box kTap{40, 18, 1, 1};
+// tap-major weights (T_WL0..T_CR2) of the 32 faces of a warp row, and of
+// the face after them (the edge-EMF sweeps on i faces, below)
+constexpr Box kTap32{32, 18, 1, 1};
+constexpr Box kTap40{40, 18, 1, 1};
 
-// Sweeps whose lanes run along i over the n+1 faces of an i row (the flux
-// along i, the EMFs along j and k) tile the row in ceil(n/32) tiles of 32
+// The edge-EMF sweeps whose lanes run along i over the n+1 faces of an i
+// row (the EMFs along j and k) tile the row in ceil(n/32) tiles of 32
 // faces; when 32 divides n the last face of the row, the upper boundary
 // face, is left over.  The last tile of the row then computes it too, in
 // one extra pass of one warp whose lanes take the tile's 8 rows (its boxes
-// are 40 wide along i, so that face's stencil is in the slot).  A ninth
-// tile would cost eight warp passes with one live lane each.
+// are 40 wide along i, so that face's stencil is in the slot), where a
+// ninth tile would cost eight warp passes with one live lane each: 1.6 %
+// off the FP64 EMF stage at 256^3 on B200.  The flux sweep along i keeps
+// its ninth tile: the same pass made it 1 % slower there (FP32 3.5 %).
 __device__ __forceinline__ bool row_end_face(const Params& P, int x0) { return x0 + 32 == NGH + P.n[0]; }
 // the warp that takes it: rotates over the row sets
 __device__ __forceinline__ int row_end_warp(const int nt[3], int t) { return (t / nt[0]) % kWarps; }
-// 1: the row-end pass is a call of its own (its registers saved around the
-// call) instead of inlined into the tile loop
-#ifndef GOP_ROWEND_NOINLINE
-#define GOP_ROWEND_NOINLINE 0
-#endif
-#if GOP_ROWEND_NOINLINE
-#define GOP_ROWEND_INLINE __noinline__
-#else
-#define GOP_ROWEND_INLINE __forceinline__
-#endif
 
-// the weights of face c of the tile (tap-major rows in shared memory)
-template <typename R>
+// the weights of one face of the tile (tap-major rows of X faces in shared
+// memory)
+template <int X, typename R>
 __device__ __forceinline__ void load_tap(const R* w, FaceWeights<R>& W) {
 #pragma unroll
   for (int u = 0; u < 7; u++) {
-    W.wl[u] = w[u * kTap.x];
-    W.wr[u] = w[(7 + u) * kTap.x];
+    W.wl[u] = w[u * X];
+    W.wr[u] = w[(7 + u) * X];
   }
-  W.cl1 = w[14 * kTap.x];
-  W.cl2 = w[15 * kTap.x];
-  W.cr1 = w[16 * kTap.x];
-  W.cr2 = w[17 * kTap.x];
+  W.cl1 = w[14 * X];
+  W.cl2 = w[15 * X];
+  W.cr1 = w[16 * X];
+  W.cr2 = w[17 * X];
 }
 
 // ------------------------------------------------------------------ flux
@@ -146,8 +140,8 @@ struct FluxTile {
   // stencil and limiter windows of the tile's faces
   static constexpr Box S = D == 0 ? Box{40, 8, 1, 1} : (D == 1 ? Box{32, 15, 1, 1} : Box{32, 1, 15, 1});
   static constexpr Box L = D == 0 ? Box{40, 8, 1, 1} : (D == 1 ? Box{32, 11, 1, 1} : Box{32, 1, 11, 1});
-  static constexpr Box WT = D == 0 ? kTap : kRec8;
-  static constexpr Box BN = D == 2 ? Box{32, 1, 8, 1} : (D == 1 ? Box{32, 8, 1, 1} : Box{40, 8, 1, 1});
+  static constexpr Box WT = D == 0 ? kTap32 : kRec8;
+  static constexpr Box BN = D == 2 ? Box{32, 1, 8, 1} : Box{32, 8, 1, 1};
   static constexpr int SB = S.elems(), LB = L.elems();
   // slot layout in elements: W_h, limiter W, mags_h, mags, weights, B_n
   static constexpr int OFF_WH = 0;
@@ -217,24 +211,11 @@ struct FluxStage {
     tma_load_4d(s + F::OFF_BN, &m.bn[par], bar, T.x0, T.y0, T.z0, D);
   }
 
-  // one face per thread; along i the last tile of a row also takes the
-  // row's upper boundary face when 32 divides n (row_end_face)
+  // one face per thread
   __device__ static void compute(const Params& P, const Work<R>& wk, const Maps& m, const R* s,
                                  int t, int warp, int lane) {
     const TileAt T = flux_at<D>(m.nt, t);
-    face(P, wk, s, T, warp, lane);
-    if constexpr (D == 0)
-      if (row_end_face(P, T.x0) && warp == row_end_warp(m.nt, t) && lane < kWarps)
-        row_end(P, wk, s, T, lane);
-  }
-  __device__ GOP_ROWEND_INLINE static void row_end(const Params& P, const Work<R>& wk, const R* s,
-                                              const TileAt T, int row) {
-    face(P, wk, s, T, row, 32);
-  }
-
-  // the face in tile row `row` (a warp's row), column `col` (a lane's face)
-  __device__ static void face(const Params& P, const Work<R>& wk, const R* s, const TileAt& T,
-                              int row, int col) {
+    const int row = warp, col = lane;
     const int i = T.x0 + col, j = T.y0 + (D == 2 ? 0 : row), k = T.z0 + (D == 2 ? row : 0);
     if (!(i < NGH + P.n[0] + (D == 0) && j < NGH + P.n[1] + (D == 1) && k < NGH + P.n[2] + (D == 2)))
       return;
@@ -255,7 +236,7 @@ struct FluxStage {
     }
     constexpr int TS = D == 0 ? 1 : 32;  // stride of one stencil tap in the slot
     FaceWeights<R> Wt;
-    if constexpr (D == 0) load_tap(s + F::OFF_W + col, Wt);
+    if constexpr (D == 0) load_tap<32>(s + F::OFF_W + col, Wt);
     else load_fw_smem(s + F::OFF_W + row * FW, Wt);
     const R bn = s[F::OFF_BN + row * F::BN.x + col];
     const R a1h = (R)(0.5 * P.pdm_a1), a2 = (R)P.pdm_a2;
@@ -300,8 +281,8 @@ struct EmfTile {
   static constexpr Box BHQ = D == 0 ? Box{32, 8, 8, 1} : (D == 1 ? Box{40, 1, 15, 1} : Box{40, 8, 1, 1});
   static constexpr Box BLQ = D == 0 ? Box{32, 4, 8, 1} : (D == 1 ? Box{40, 1, 11, 1} : Box{40, 8, 1, 1});
   static constexpr Box RHO = D == 0 ? Box{32, 2, 9, 1} : (D == 1 ? Box{40, 1, 9, 1} : Box{40, 9, 1, 1});
-  static constexpr Box WQ = D == 1 ? kTap : kRec8;
-  static constexpr Box WP = D == 0 ? kRec1 : (D == 1 ? kRec8 : kTap);
+  static constexpr Box WQ = D == 1 ? kTap40 : kRec8;
+  static constexpr Box WP = D == 0 ? kRec1 : (D == 1 ? kRec8 : kTap40);
   static constexpr int VF = V.x * V.y * V.z;  // elements of one V field
   static constexpr int OFF_V = 0;
   static constexpr int OFF_BHP = OFF_V + V.padded();
@@ -397,8 +378,8 @@ struct EmfStage {
       if (row_end_face(P, T.x0) && warp == row_end_warp(m.nt, t) && lane < kWarps)
         row_end(P, wk, s, T, lane);
   }
-  __device__ GOP_ROWEND_INLINE static void row_end(const Params& P, const Work<R>& wk, const R* s,
-                                              const TileAt T, int row) {
+  __device__ __forceinline__ static void row_end(const Params& P, const Work<R>& wk, const R* s,
+                                                const TileAt T, int row) {
     edge(P, wk, s, T, row, 32);
   }
 
@@ -439,7 +420,7 @@ struct EmfStage {
       // (i-1,k-1) + (i-1,k) + (i,k-1) + (i,k); box rows of 40 along k
       const R* r = rh + lane + 3;
       rho4 = r[warp * 40] + r[(warp + 1) * 40] + r[warp * 40 + 1] + r[(warp + 1) * 40 + 1];
-      load_tap(s + E::OFF_WQ + lane, Wq);
+      load_tap<40>(s + E::OFF_WQ + lane, Wq);
       load_fw_smem(s + E::OFF_WP + warp * FW, Wp);
     } else {  // q = j rows of 40; p = i in a row of 40
       v0 = s + E::OFF_V + warp * 40 + lane;
@@ -451,7 +432,7 @@ struct EmfStage {
       const R* r = rh + lane + 3;
       rho4 = r[warp * 40] + r[(warp + 1) * 40] + r[warp * 40 + 1] + r[(warp + 1) * 40 + 1];
       load_fw_smem(s + E::OFF_WQ + warp * FW, Wq);
-      load_tap(s + E::OFF_WP + lane, Wp);
+      load_tap<40>(s + E::OFF_WP + lane, Wp);
     }
     R vav[2], bpL, bpR, bqL, bqR;
 #pragma unroll
@@ -663,7 +644,7 @@ static bool field_map(CUtensorMap* m, const R* base, int nf, const Params& P, co
 template <typename R>
 static bool weight_map(CUtensorMap* m, const Work<R>& w, const Params& P, const Box& b) {
   const cuuint64_t es = sizeof(R), tm = (cuuint64_t)P.tmax;
-  if (b.x == kTap.x && b.y == kTap.y) {
+  if (b.y == kTap32.y && (b.x == kTap32.x || b.x == kTap40.x)) {
     const cuuint64_t d[4] = {tm, (cuuint64_t)NTAB, 3, 1};
     const cuuint64_t st[3] = {tm * es, tm * NTAB * es, tm * NTAB * 3 * es};
     return encode<R>(m, w.tab, d, st, b);
@@ -695,8 +676,8 @@ static bool make_flux_maps(FluxMaps& m, const Params& P, const Work<R>& w) {
     ok = field_map<R>(&m.wl[b], lim_state<R>(P, w, b), 6, P, L5) &&
          field_map<R>(&m.bn[b], lim_face<R>(P, w, b), 3, P, F::BN);
   const int n0 = P.n[0], n1 = P.n[1], n2 = P.n[2];
-  if (D == 0) {  // i-face tiles (the row-end face in the last), j-row tiles, k planes
-    m.nt[0] = (n0 + 31) / 32;
+  if (D == 0) {  // i-face tiles, j-row tiles, k planes
+    m.nt[0] = (n0 + 1 + 31) / 32;
     m.nt[1] = (n1 + 7) / 8;
     m.nt[2] = n2;
   } else if (D == 1) {  // i tiles, j-face tiles, k planes
@@ -725,11 +706,11 @@ static bool make_emf_maps(EmfMaps& m, const Params& P, const Work<R>& w) {
     m.nt[0] = (n0 + 31) / 32;
     m.nt[1] = (n2 + 1 + 7) / 8;
     m.nt[2] = n1 + 1;
-  } else if (D == 1) {  // i-face tiles (row-end face as for the flux), k-face tiles, j cells
+  } else if (D == 1) {  // i-face tiles (the row-end face in the last), k-face tiles, j cells
     m.nt[0] = (n0 + 31) / 32;
     m.nt[1] = (n2 + 1 + 7) / 8;
     m.nt[2] = n1;
-  } else {  // i-face tiles (row-end face as for the flux), j-face tiles, k cells
+  } else {  // i-face tiles (the row-end face in the last), j-face tiles, k cells
     m.nt[0] = (n0 + 31) / 32;
     m.nt[1] = (n1 + 1 + 7) / 8;
     m.nt[2] = n2;

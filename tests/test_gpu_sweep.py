@@ -76,7 +76,7 @@ CASES = [
          dom=(1.0, 2.0, 0.25 * math.pi, 0.75 * math.pi, -0.25 * math.pi, 0.25 * math.pi),
          coord=2, bc="eeeeee", kind="loop_sph", prec=1, steps=12),
     # ni a multiple of 32: the i rows' upper boundary faces come with the
-    # last tile of each row (the row-end pass of the i-face sweeps)
+    # last tile of each row (the row-end pass of the EMF sweeps on i faces)
     dict(id="blast_64x48x40_mixed", n=(64, 48, 40), dom=(-0.5, 0.5) * 3, coord=0, bc="pppppp",
          kind="blast", prec=1, steps=12),
     dict(id="sphere_96x35x19", n=(96, 35, 19),
