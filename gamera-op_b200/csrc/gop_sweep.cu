@@ -114,8 +114,11 @@ constexpr Box kTap40{40, 18, 1, 1};
 // off the FP64 EMF stage at 256^3 on B200.  The flux sweep along i keeps
 // its ninth tile: the same pass made it 1 % slower there (FP32 3.5 %).
 __device__ __forceinline__ bool row_end_face(const Params& P, int x0) { return x0 + 32 == NGH + P.n[0]; }
-// the warp that takes it: rotates over the row sets
-__device__ __forceinline__ int row_end_warp(const int nt[3], int t) { return (t / nt[0]) % kWarps; }
+// the warp that takes it: rotates over the row sets (kWarps a power of 2)
+template <class T>
+__device__ __forceinline__ int row_end_warp(const int nt[3], const T& t) {
+  return (t.b + nt[1] * t.c) & (kWarps - 1);
+}
 
 // the weights of one face of the tile (tap-major rows of X faces in shared
 // memory)
@@ -172,9 +175,30 @@ struct alignas(64) FluxMaps {
 struct TileAt {
   int x0, y0, z0;
 };
+// A tile index t = a + nt[0] * (b + nt[1] * c) as its three digits.  The
+// blocks walk the tiles in steps of the grid size, and adding the step's
+// digits with carries replaces the divisions by nt of every tile (about a
+// hundred integer instructions per thread and tile).
+struct Tile {
+  int a, b, c;
+};
+__device__ __forceinline__ Tile tile_of(const int nt[3], int t) {
+  const int r = t / nt[0];
+  return {t % nt[0], r % nt[1], r / nt[1]};
+}
+// p += s (s's digits below nt: one carry per digit at most)
+__device__ __forceinline__ void tile_add(Tile& p, const Tile& s, const int nt[3]) {
+  p.a += s.a;
+  int carry = p.a >= nt[0];
+  if (carry) p.a -= nt[0];
+  p.b += s.b + carry;
+  carry = p.b >= nt[1];
+  if (carry) p.b -= nt[1];
+  p.c += s.c + carry;
+}
 template <int D>
-__device__ __forceinline__ TileAt flux_at(const int nt[3], int t) {
-  const int a = t % nt[0], r = t / nt[0], b = r % nt[1], c = r / nt[1];
+__device__ __forceinline__ TileAt flux_at(const Tile& p) {
+  const int a = p.a, b = p.b, c = p.c;
   TileAt T;
   T.x0 = NGH + 32 * a;
   if constexpr (D == 2) {  // warps: faces along k, one row j
@@ -195,8 +219,9 @@ struct FluxStage {
   static constexpr int ELEMS = F::ELEMS;
   static constexpr int TX = F::TX;
 
-  __device__ static void issue(const Params& P, const Maps& m, int par, int t, R* s, uint64_t* bar) {
-    const TileAt T = flux_at<D>(m.nt, t);
+  __device__ static void issue(const Params& P, const Maps& m, int par, const Tile& t, R* s,
+                               uint64_t* bar) {
+    const TileAt T = flux_at<D>(t);
     const int f0 = D == 0 ? T.x0 : (D == 1 ? T.y0 : T.z0);  // first face along D
     // stencil windows start 4 cells before the first face, limiter windows
     // 2 (along i both start 4 before, keeping x aligned)
@@ -213,8 +238,8 @@ struct FluxStage {
 
   // one face per thread
   __device__ static void compute(const Params& P, const Work<R>& wk, const Maps& m, const R* s,
-                                 int t, int warp, int lane) {
-    const TileAt T = flux_at<D>(m.nt, t);
+                                 const Tile& t, int warp, int lane) {
+    const TileAt T = flux_at<D>(t);
     const int row = warp, col = lane;
     const int i = T.x0 + col, j = T.y0 + (D == 2 ? 0 : row), k = T.z0 + (D == 2 ? row : 0);
     if (!(i < NGH + P.n[0] + (D == 0) && j < NGH + P.n[1] + (D == 1) && k < NGH + P.n[2] + (D == 2)))
@@ -311,8 +336,8 @@ struct alignas(64) EmfMaps {
 };
 
 template <int D>
-__device__ __forceinline__ TileAt emf_at(const int nt[3], int t) {
-  const int a = t % nt[0], r = t / nt[0], b = r % nt[1], c = r / nt[1];
+__device__ __forceinline__ TileAt emf_at(const Tile& p) {
+  const int a = p.a, b = p.b, c = p.c;
   TileAt T;
   T.x0 = NGH + 32 * a;
   if constexpr (D == 2) {  // warps: faces along j, one plane k
@@ -334,8 +359,9 @@ struct EmfStage {
   static constexpr int TX = E::TX;
   static constexpr int p = (D + 1) % 3, q = (D + 2) % 3;
 
-  __device__ static void issue(const Params& P, const Maps& m, int par, int t, R* s, uint64_t* bar) {
-    const TileAt T = emf_at<D>(m.nt, t);
+  __device__ static void issue(const Params& P, const Maps& m, int par, const Tile& t, R* s,
+                               uint64_t* bar) {
+    const TileAt T = emf_at<D>(t);
     const int x0 = T.x0, y0 = T.y0, z0 = T.z0;
     if constexpr (D == 0) {  // i cells, j face y0, k faces z0..
       tma_load_4d(s + E::OFF_V, &m.v, bar, x0, y0, z0 - 4, 0);
@@ -371,8 +397,8 @@ struct EmfStage {
   // the row's upper boundary face in the last tile of a row when 32
   // divides n (row_end_face)
   __device__ static void compute(const Params& P, const Work<R>& wk, const Maps& m, const R* s,
-                                 int t, int warp, int lane) {
-    const TileAt T = emf_at<D>(m.nt, t);
+                                 const Tile& t, int warp, int lane) {
+    const TileAt T = emf_at<D>(t);
     edge(P, wk, s, T, warp, lane);
     if constexpr (D != 0)
       if (row_end_face(P, T.x0) && warp == row_end_warp(m.nt, t) && lane < kWarps)
@@ -521,26 +547,28 @@ __device__ __forceinline__ void sweep_run(const Params& P, const Work<R>& wk,
   uint64_t* empty = full + S;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const bool feeder = threadIdx.x == 0;
-  const int ntiles = maps.nt[0] * maps.nt[1] * maps.nt[2];
+  const int nt2 = maps.nt[2];  // tiles run out when the third digit reaches it
   const int par = sizeof(R) == 8 ? cur_buf(P) : 0;
-  auto issue = [&](int n, int t) {
+  auto issue = [&](int n, const Tile& t) {
     const int q = n % S;
     mbar_arrive_expect_tx(&full[q], TXB);
     Stage::issue(P, maps, par, t, slots + (size_t)q * Stage::ELEMS, &full[q]);
   };
-  int issued = 0;  // feeder only: tiles whose copies were issued
+  const Tile step = tile_of(maps.nt, gridDim.x);
+  Tile next = tile_of(maps.nt, blockIdx.x);  // feeder only: the first tile not yet issued
+  int issued = 0;                            // feeder only: tiles whose copies were issued
   if (feeder) {
     for (int q = 0; q < S; q++) {
       mbar_init(&full[q], 1);
       mbar_init(&empty[q], kWarps);
     }
     fence_mbar_init();
-    for (int t = blockIdx.x; t < ntiles && issued < S; t += gridDim.x) issue(issued++, t);
+    for (; next.c < nt2 && issued < S; tile_add(next, step, maps.nt)) issue(issued++, next);
   }
   __syncthreads();
   bool ok = true;
   int n = 0;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, n++) {
+  for (Tile t = tile_of(maps.nt, blockIdx.x); t.c < nt2; tile_add(t, step, maps.nt), n++) {
     const int q = n % S;
     const uint32_t ph = (n / S) & 1;
     if (!mbar_wait(&full[q], ph)) {
@@ -550,16 +578,14 @@ __device__ __forceinline__ void sweep_run(const Params& P, const Work<R>& wk,
     Stage::compute(P, wk, maps, slots + (size_t)q * Stage::ELEMS, t, warp, lane);
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[q]);
-    if (feeder) {
-      const int tn = t + S * (int)gridDim.x;
-      if (tn < ntiles) {
-        // every warp has released this slot: refill it with the tile S ahead
-        if (!mbar_wait(&empty[q], ph)) {
-          ok = false;
-          break;
-        }
-        issue(issued++, tn);
+    if (feeder && next.c < nt2) {
+      // every warp has released this slot: refill it with the tile S ahead
+      if (!mbar_wait(&empty[q], ph)) {
+        ok = false;
+        break;
       }
+      issue(issued++, next);
+      tile_add(next, step, maps.nt);
     }
   }
   if (feeder) {
