@@ -949,6 +949,81 @@ __device__ __forceinline__ void wrap_body(const Params& P, int axis, int which, 
   }
 }
 
+// All three axes periodic: the three wraps above in one launch.  The three
+// in turn leave at every ghost point the value of the active point reached
+// by wrapping each of its ghost coordinates (x + n below the active range,
+// x - n above it): each later wrap copies what the earlier ones wrote, edges
+// and corners included.  Thread g runs over three slabs, axis a's 9 layers
+// (4 ghost layers below, 5 points above: the cell fields' 4 ghost layers
+// and the padding point, or the upper boundary face and the face field's 4
+// ghost layers) times all points of the other two axes; a (point, field)
+// pair is written by the slab of its lowest ghost axis only, so once, and
+// no thread writes a point that another reads (sources have no ghost
+// coordinate).
+__device__ __forceinline__ void wrap3_body(const Params& P, int which, long long g) {
+  const long long N0 = P.N[0], N1 = P.N[1], N2 = P.N[2];
+  const long long s0 = 9 * N1 * N2, s1 = N0 * 9 * N2, s2 = N0 * N1 * 9;
+  int a, x[3];
+  if (g < s0) {
+    a = 0;
+    x[0] = (int)(g % 9);
+    const long long r = g / 9;
+    x[1] = (int)(r % N1);
+    x[2] = (int)(r / N1);
+  } else if (g < s0 + s1) {
+    a = 1;
+    const long long r = g - s0;
+    x[0] = (int)(r % N0);
+    x[1] = (int)((r / N0) % 9);
+    x[2] = (int)(r / N0 / 9);
+  } else if (g < s0 + s1 + s2) {
+    a = 2;
+    const long long r = g - s0 - s1;
+    x[0] = (int)(r % N0);
+    x[1] = (int)((r / N0) % N1);
+    x[2] = (int)(r / N0 / N1);
+  } else {
+    return;
+  }
+  if (x[a] >= NGH) x[a] += P.n[a];  // the 5 points above the active range
+  const int bsel = which ? cur_buf(P) : 1 - cur_buf(P);
+  double* __restrict__ W = P.Wbuf[bsel];
+  double* __restrict__ B = P.Bbuf[bsel];
+  const bool ps = P.ps_live != 0;  // p_S zero everywhere stays so: skipped
+  long long src[9], dst[9];
+  bool on[9];
+#pragma unroll
+  for (int f = 0; f < 9; f++) {
+    int y[3] = {x[0], x[1], x[2]};
+    int low = 3;  // lowest ghost axis of this field at this point
+#pragma unroll
+    for (int b = 2; b >= 0; b--) {
+      const int o = (f >= 6 && f - 6 == b) ? 1 : 0;  // the face field along b
+      if (y[b] < NGH) {
+        y[b] += P.n[b];
+        low = b;
+      } else if (y[b] >= NGH + P.n[b] + o && y[b] < 2 * NGH + P.n[b] + o) {
+        y[b] -= P.n[b];
+        low = b;
+      }
+    }
+    on[f] = low == a && (f != PS || ps);
+    src[f] = lin(P, y[0], y[1], y[2]);
+    dst[f] = lin(P, x[0], x[1], x[2]);
+  }
+  double v[9];
+#pragma unroll
+  for (int f = 0; f < 9; f++) {
+    const double* q = f < 6 ? W + (size_t)f * P.fs : B + (size_t)(f - 6) * P.fs;
+    if (on[f]) v[f] = q[src[f]];
+  }
+#pragma unroll
+  for (int f = 0; f < 9; f++) {
+    double* q = f < 6 ? W + (size_t)f * P.fs : B + (size_t)(f - 6) * P.fs;
+    if (on[f]) q[dst[f]] = v[f];
+  }
+}
+
 // One face of the ghost-fill library (src/boundary_conditions.c): the 6 gas
 // primitives with kind `kind` (gas_bc_*) and the 3 face fields with kind
 // `gkind` (gem_bc_*); 0 skips that group.  t = (i, j, k) with the
@@ -1003,6 +1078,12 @@ __device__ __forceinline__ void bcface_body(const Params& P, int axis, int side,
 }
 
 // ------------------------------------------------- single-instance kernels
+
+// 1: a fully periodic grid fills its ghosts in one launch (k_wrap3) instead
+// of one per axis
+#ifndef GOP_WRAP3
+#define GOP_WRAP3 1
+#endif
 
 // Resident 256-thread blocks per SM each kernel is compiled for (caps its
 // registers at 65536 / (256 * n)), per stage and arithmetic type; the
@@ -1172,6 +1253,11 @@ __global__ void k_wrap(Params P, int axis, int which) {
   pdl_enter();
   if (stopped(P)) return;
   wrap_body(P, axis, which, grid_pos());
+}
+__global__ void k_wrap3(Params P, int which) {
+  pdl_enter();
+  if (stopped(P)) return;
+  wrap3_body(P, which, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 __global__ void k_bcface(Params P, int axis, int side, int kind, int gkind, int which) {
   pdl_enter();
@@ -1452,6 +1538,12 @@ void launch_ghosts(const Params& P, const char bc[6], const char gem_bc[6], int 
                    cudaStream_t st) {
   bool periodic[3];
   for (int a = 0; a < 3; a++) periodic[a] = bc[2 * a] == 'p' && bc[2 * a + 1] == 'p';
+  if (periodic[0] && periodic[1] && periodic[2] && GOP_WRAP3) {
+    const long long N0 = P.N[0], N1 = P.N[1], N2 = P.N[2];
+    const long long pts = 9 * (N1 * N2 + N0 * N2 + N0 * N1);
+    LAUNCH(k_wrap3, dim3((unsigned)((pts + 255) / 256)), dim3(256), st, P, which);
+    return;
+  }
   for (int a = 0; a < 3; a++) {
     if (!periodic[a]) continue;
     const dim3 sp = launch_space(P, K_WRAP0 + a), blk = ghost_block(K_WRAP0 + a);
