@@ -2,8 +2,8 @@
 
 Small cases compare against the golden vectors of GAMERA-OP's own solver and
 against the C restatement in oracle/ on the same inputs; the plain FP64 path
-must agree to relative L1 <= 1e-10 per variable (the bar of the north star,
-after 100 steps on the Orszag-Tang case).  Size-independent properties (div B
+must agree to relative L1 <= 1e-10 per variable (the parity bar of this
+path, after 100 steps on the Orszag-Tang case).  Size-independent properties (div B
 at round-off, exact mass conservation in periodic boxes, determinism,
 restart equivalence) cover larger grids.
 """
