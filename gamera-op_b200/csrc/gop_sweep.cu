@@ -12,15 +12,16 @@
 // address arithmetic and latency, not the FP64 arithmetic, bound them.
 // Here each block is persistent and runs a copy pipeline:
 //
-//   copies   one elected thread streams tiles into a ring of STAGES
-//            shared-memory slots with cp.async.bulk.tensor (one TMA box per
+//   copies   one elected thread streams tiles into a ring of 2-4
+//            shared-memory slots (as many as fit the SM at the kernel's
+//            residency) with cp.async.bulk.tensor (one TMA box per
 //            input array and tile: stencil windows, limiter windows, PDM
 //            weights), completing on the slot's "full" mbarrier;
 //   compute  8 warps compute one face or edge per thread from shared memory
 //            (every stencil tap is a load at a compile-time offset from one
 //            per-thread base) and release the slot on its "empty" mbarrier;
-//            the feeding thread refills a released slot with the tile
-//            STAGES ahead.
+//            the feeding thread refills a released slot with the next tile
+//            not yet issued, a ring's length ahead.
 //
 // So the global-memory latency of tile n+1 overlaps the arithmetic of tile
 // n, and the stencil re-reads come from shared memory instead of L1.  The
@@ -50,8 +51,9 @@ namespace gop {
 constexpr int kWarps = 8;
 constexpr int kSweepThreads = 32 * kWarps;
 
-// shared-memory ring and residency per arithmetic type: two slots and two
-// blocks per SM in FP64 (128 registers), two slots and three blocks in FP32
+// shared-memory ring and residency per arithmetic type: at least two slots;
+// two blocks per SM in FP64 (128 registers), three in FP32 (the flux; the
+// EMF below)
 #ifndef GOP_SWEEP_STAGES_F64
 #define GOP_SWEEP_STAGES_F64 2
 #endif
