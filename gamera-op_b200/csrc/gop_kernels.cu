@@ -1235,6 +1235,17 @@ __global__ void __launch_bounds__(256, GOP_MINB(FLUX, R)) k_flux(Params P, Work<
   if (stopped(P)) return;
   flux_body<R, D, BG, PSL>(P, w, grid_pos());
 }
+// The faces i = NGH + n0 (the upper boundary face of every i row) of the
+// flux along i, one thread per (j, k) row: the i sweep leaves them out when
+// 32 divides n0 (a ninth tile of 32 lanes per row would run with one live
+// lane per warp)
+template <typename R, bool BG>
+__global__ void __launch_bounds__(256) k_flux_col(Params P, Work<R> w) {
+  pdl_enter();
+  if (stopped(P)) return;
+  const int tj = blockIdx.x * blockDim.x + threadIdx.x, tk = blockIdx.y * blockDim.y + threadIdx.y;
+  flux_body<R, 0, BG, false>(P, w, Pos{P.n[0], tj, tk});
+}
 template <int COORD, typename R>
 __global__ void __launch_bounds__(256, GOP_MINB_CT) k_ct(Params P, Work<R> w) {
   pdl_enter();
@@ -1466,6 +1477,17 @@ static void launch_slot_bg(const Params& P, int coord, const Work<R>& w, int slo
     default: break;
   }
 }
+
+template <typename R>
+void launch_flux_col(const Params& P, const Work<R>& w, cudaStream_t st) {
+  const dim3 blk(32, 8, 1);
+  const dim3 g((P.n[1] + 31) / 32, (P.n[2] + 7) / 8, 1);
+  // right after a sweep: no early launch (see launch_step_body)
+  if (P.bg) LAUNCH_PDL(false, (k_flux_col<R, true>), g, blk, st, P, w);
+  else LAUNCH_PDL(false, (k_flux_col<R, false>), g, blk, st, P, w);
+}
+template void launch_flux_col<double>(const Params&, const Work<double>&, cudaStream_t);
+template void launch_flux_col<float>(const Params&, const Work<float>&, cudaStream_t);
 
 template <typename R>
 void launch_slot(const Params& P, int coord, const Work<R>& w, int slot, dim3 blk,

@@ -65,6 +65,10 @@ void sweep_destroy(SweepSet* s);
 template <typename R>
 bool launch_flux_sweep(const SweepSet* sw, const Params& P, const Work<R>& w, int D,
                        cudaStream_t st);
+// the row-end faces of the flux along i that its sweep leaves out (32
+// dividing n0), by the per-face arithmetic
+template <typename R>
+void launch_flux_col(const Params& P, const Work<R>& w, cudaStream_t st);
 // the EMF of the edges along D by the sweep kernel; false without maps
 template <typename R>
 bool launch_emf_sweep(const SweepSet* sw, const Params& P, const Work<R>& w, int D,
